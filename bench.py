@@ -1,0 +1,306 @@
+#!/usr/bin/env python3
+"""Benchmark of the FSP generator action y += A(t) x (the hot path) on B200.
+
+Workload: mass_action_3 -- 3 species, 9 mass-action reactions, box 255^3 = 16,777,216 states,
+KRONECKER (matrix-free, factorised) format, FP64.  One step = one application of the generator to
+the full state vector through the C ABI (cufsp_mat_apply, accumulate form).
+
+  value     algorithmic HBM GB/s = 24 B/state * states / time (x read once, y read + written),
+            device-resident inputs, CUDA events on the launching stream, summed over ranks
+  e2e       the same metric through cufsp_mat_action_host with pinned HOST x, y: H2D of x and y and
+            D2H of y inside the timed region
+  roofline  the kernel's achieved GB/s against the measured HBM copy bandwidth
+  cpu_baseline  the FP64 host oracle (OpenMP CSR SpMV restating the reference's assembly) timed on
+            the host cores on a bounded sample (box 255 x 255 x 63, about 10 s)
+  secondary expmv solves/s on birth_death_2 (32,768 states, t = 10, m = 30, tol 1e-8)
+
+--impl reference: the reference has no CPU implementation of this path; its CPU restatement (the
+oracle, "port") is timed on the same metric and workload sample with all host threads.
+Multi-GPU (--gpus N under torchrun): the action of one generator does not shard, so every rank
+runs an independent replica (weak scaling); time = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "matvec HBM GB/s; expmv solves/s & ∇logL grads/s at 1e-8 err vs plain FSP"
+BYTES_PER_STATE = 24
+WORKLOAD = ("mass_action_3 generator action y += A(t)x: 3 species, 9 reactions, box 255^3 = 16,777,216 states, "
+            "KRONECKER matrix-free, FP64")
+CPU_SAMPLE_BOUNDS = (255, 255, 63)
+
+
+def measured_peak_hbm() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+def profile_traffic() -> float | None:
+    """DRAM bytes per launch of the KRONECKER action from the committed ncu summary, if present."""
+    p = ROOT / "profiles" / "kron_mv_mass_action_3.md"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.strip().startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].strip().split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.t.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_oracle_gbs(min_steps: int, warmup: int, bounds=CPU_SAMPLE_BOUNDS, budget_s: float = 10.0) -> dict:
+    """Time the oracle's OpenMP CSR SpMV (y += A x) on a bounded sample of the workload: at least
+    `min_steps` steps and about `budget_s` seconds of CPU work."""
+    import oracle
+    from cuda_fsp_b200 import models
+    m = models.mass_action_3(bounds=bounds)
+    csr = oracle.assemble_model(m)
+    rng = np.random.default_rng(0)
+    x = rng.uniform(0, 1, m.n_states)
+    y = np.zeros(m.n_states)
+    c = m.coefs(0)
+    for _ in range(max(1, warmup)):
+        y = csr.spmv(c, x, y, beta=1.0)
+    steps = 0
+    t0 = time.perf_counter()
+    while steps < min_steps or time.perf_counter() - t0 < budget_s:
+        y = csr.spmv(c, x, y, beta=1.0)
+        steps += 1
+    dt = (time.perf_counter() - t0) / steps
+    return {"value": BYTES_PER_STATE * m.n_states / dt / 1e9, "unit": "GB/s", "cores": oracle.num_threads(),
+            "kind": "port", "sample": f"oracle CSR SpMV y += A x on box {bounds[0]}x{bounds[1]}x{bounds[2]} "
+                                      f"({m.n_states} states, same 9-reaction model), {steps} steps",
+            "ms_per_step": dt * 1e3}
+
+
+def run_reference(args):
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return
+    steps = max(1, args.steps)
+    cb = cpu_oracle_gbs(steps, max(1, min(args.warmup, 2)))
+    line = {"impl": "reference", "metric": METRIC, "value": round(cb["value"], 3), "unit": "GB/s",
+            "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup, "ms_per_step": round(cb["ms_per_step"], 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": WORKLOAD, "sample": cb["sample"]},
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": round(cb["value"], 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def expmv_secondary() -> dict:
+    import torch
+    from cuda_fsp_b200 import FSPMat, KryExpvFSP, MatrixFormat, models
+    m = models.birth_death_2()
+    A = FSPMat.from_model(m, MatrixFormat.KRONECKER)
+    p0 = torch.as_tensor(m.p0(), device="cuda")
+    c = m.coefs(0)
+    v = p0.clone()
+    KryExpvFSP(10.0, A, v, m=30, tol=1e-8, coefs=c).solve()  # warm-up
+    reps = 3
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    st = None
+    for _ in range(reps):
+        v.copy_(p0)
+        st = KryExpvFSP(10.0, A, v, m=30, tol=1e-8, coefs=c).solve()
+    torch.cuda.synchronize()
+    dt = (time.perf_counter() - t0) / reps
+    return {"metric": "expmv solves/s", "workload": "birth_death_2, 32,768 states, t = 10, m = 30, tol 1e-8",
+            "value": round(1.0 / dt, 3), "ms_per_solve": round(dt * 1e3, 3), "krylov_steps": st["n_steps"],
+            "matvecs": st["n_matvec"]}
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from cuda_fsp_b200 import FSPMat, MatrixFormat, models
+
+    world, rank, local = dist_setup()
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=300))
+    dev = torch.device("cuda", local if world > 1 else 0)
+    torch.cuda.set_device(dev)
+
+    m = models.mass_action_3()
+    n = m.n_states
+    A = FSPMat.from_model(m, MatrixFormat.KRONECKER)
+    c = m.coefs(0)
+    n_sets = 4  # rotate 4 (x, y) pairs = 1.07 GB > 126 MB L2 between timed iterations
+    g = torch.Generator(device=dev).manual_seed(1234 + rank)
+    xs = [torch.rand(n, dtype=torch.float64, device=dev, generator=g) for _ in range(n_sets)]
+    ys = [torch.zeros(n, dtype=torch.float64, device=dev) for _ in range(n_sets)]
+    stream = torch.cuda.current_stream(dev)
+
+    def step(i):
+        A.apply(xs[i % n_sets], ys[i % n_sets], coefs=c, beta=1.0, stream=stream.cuda_stream)
+
+    for i in range(max(3, args.warmup)):
+        step(i)
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    time.sleep(0.3)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    ev0.record(stream)
+    for i in range(args.steps):
+        step(i)
+    ev1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = ev0.elapsed_time(ev1) / args.steps
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = t.item()
+        dist.barrier()
+    clk = clocks.stop()
+    kernel_gbs = BYTES_PER_STATE * n / (ms * 1e-3) / 1e9
+    value = kernel_gbs * world
+
+    # e2e through the host-buffer entry point (pinned host memory, copies inside the timed region)
+    xh = torch.empty(n, dtype=torch.float64).pin_memory()
+    yh = torch.empty(n, dtype=torch.float64).pin_memory()
+    xh.copy_(xs[0].cpu())
+    yh.zero_()
+    e2e_steps = max(2, min(args.steps, 10))
+    A.action_host(0.0, xh, yh)
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        A.action_host(0.0, xh, yh)
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    if world > 1:
+        t = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = t.item()
+    e2e_gbs = BYTES_PER_STATE * n / e2e_s / 1e9 * world
+
+    secondary = expmv_secondary() if rank == 0 else None
+    cpu = cpu_oracle_gbs(max(3, min(args.steps, 20)), 1) if (rank == 0 and world == 1) else None
+    peak, peak_kind = measured_peak_hbm()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms, 5), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "n_states": n, "format": "KRONECKER", "form": "y += A x",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "l2": "4 rotating (x, y) input pairs, 1.07 GB > 126 MB L2",
+                       "bytes_per_state": BYTES_PER_STATE},
+            "e2e": {"value": round(e2e_gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": 16 * n, "d2h_bytes_per_step": 8 * n,
+                    "entry_point": "cufsp_mat_action_host", "ms_per_step": round(e2e_s * 1e3, 3)},
+            "roofline": {"bound": "hbm", "achieved": round(kernel_gbs, 3), "peak": peak, "unit": "GB/s",
+                         "frac": round(kernel_gbs / peak, 4), "traffic": profile_traffic(),
+                         "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured" else "fallback 6.65 TB/s",
+                         "kernel": "k_kron_mv (cufsp_kron.cu)"},
+            "cpu_baseline": ({k: (round(v, 3) if isinstance(v, float) else v) for k, v in cpu.items() if k != "ms_per_step"}
+                             if cpu else None),
+            "clocks": clk,
+            "gpu_launches": args.steps,
+            "secondary": secondary,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,11 @@
+"""cuda_fsp_b200 -- B200-native (sm_100a, FP64) Finite State Projection engine.
+
+The product is the CUDA library behind include/cufsp.h (cuda_fsp_b200/lib/libcufsp.so); this
+package is its Python mirror of the reference's API (FSPMat, KryExpvFSP) plus the workload
+definitions in `models`.
+"""
+from . import models
+from ._lib import CufspError
+from .fsp import FSPMat, KryExpvFSP, MatrixFormat, expm, get_states, num_states
+
+__all__ = ["models", "CufspError", "FSPMat", "KryExpvFSP", "MatrixFormat", "expm", "get_states", "num_states"]

@@ -1,0 +1,316 @@
+// cufsp_common.cu -- status handling, state indexing and enumeration, model validation,
+// and the basic deterministic vector reductions used by the Krylov driver.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+
+#include "cufsp_internal.h"
+#include "cufsp_reduce.cuh"
+
+namespace cufsp {
+
+static thread_local std::string g_last_error;
+
+cufsp_status set_error(cufsp_status s, const std::string &msg) {
+    g_last_error = msg;
+    return s;
+}
+
+cufsp_status cuda_error(cudaError_t e, const char *what) {
+    cudaGetLastError();  // clear a sticky-free error so later calls are not misreported
+    std::string m = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+    if (e == cudaErrorMemoryAllocation) return set_error(CUFSP_ERR_ALLOC, m);
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver || e == cudaErrorNoKernelImageForDevice)
+        return set_error(CUFSP_ERR_NO_DEVICE, m);
+    return set_error(CUFSP_ERR_CUDA, m);
+}
+
+void clear_error() { g_last_error.clear(); }
+
+const DeviceInfo &device_info() {
+    static std::mutex mu;
+    static std::vector<DeviceInfo> cache;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(mu);
+    if ((int)cache.size() <= dev) cache.resize(dev + 1);
+    DeviceInfo &d = cache[dev];
+    if (d.sm_count == 0) {
+        cudaDeviceGetAttribute(&d.sm_count, cudaDevAttrMultiProcessorCount, dev);
+        cudaDeviceGetAttribute(&d.max_smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        if (d.sm_count <= 0) d.sm_count = 148;
+    }
+    return d;
+}
+
+FastDiv make_fastdiv(uint32_t d) {
+    FastDiv f;
+    f.d = d;
+    uint32_t l = 0;
+    while ((1ull << l) < d) ++l;
+    f.shift = l;
+    f.mul = (uint32_t)((((1ull << 32) * ((1ull << l) - d)) / d) + 1ull);
+    return f;
+}
+
+int stream_grid(int64_t n, int elems_per_thread, int max_ctas) {
+    int64_t per_cta = (int64_t)kRedThreads * elems_per_thread;
+    int64_t g = (n + per_cta - 1) / per_cta;
+    if (g < 1) g = 1;
+    if (g > max_ctas) g = max_ctas;
+    return (int)g;
+}
+
+cufsp_status ReduceScratch::init(int ctas, int k) {
+    release();
+    max_ctas = ctas;
+    max_k = k;
+    CUFSP_CUDA_TRY(cudaMalloc(&partials, sizeof(double) * (size_t)ctas * k));
+    CUFSP_CUDA_TRY(cudaMalloc(&counter, sizeof(unsigned int) * 4));
+    CUFSP_CUDA_TRY(cudaMemset(counter, 0, sizeof(unsigned int) * 4));
+    return CUFSP_SUCCESS;
+}
+
+void ReduceScratch::release() {
+    if (partials) cudaFree(partials);
+    if (counter) cudaFree(counter);
+    partials = nullptr;
+    counter = nullptr;
+}
+
+// ---- kernels ---------------------------------------------------------------------------------
+
+struct DecodeArgs {
+    int ns;
+    FastDiv div[CUFSP_MAX_SPECIES];
+};
+
+// fsp_get_states (src/cme_util.cu:24-41).  Each CTA decodes 256 consecutive states into shared
+// memory and writes them out as one contiguous, coalesced block of 256*ns ints.
+__global__ void __launch_bounds__(256) k_get_states(DecodeArgs a, int n, int *__restrict__ out) {
+    extern __shared__ int sm_states[];
+    const int64_t base = (int64_t)blockIdx.x * 256;
+    const int i = (int)(base + threadIdx.x);
+    if (i < n) {
+        uint32_t rem = (uint32_t)i;
+        for (int s = 0; s < a.ns; ++s) {
+            uint32_t q = fd_div(rem, a.div[s]);
+            sm_states[threadIdx.x * a.ns + s] = (int)(rem - q * a.div[s].d);
+            rem = q;
+        }
+    }
+    __syncthreads();
+    const int64_t count = min((int64_t)256, (int64_t)n - base) * a.ns;
+    int *dst = out + base * a.ns;
+    for (int t = threadIdx.x; t < count; t += 256) dst[t] = sm_states[t];
+}
+
+template <int KP>
+__global__ void __launch_bounds__(kRedThreads) k_sum(int64_t n, const double *__restrict__ x, bool squares,
+                                                     double *__restrict__ partials, unsigned int *__restrict__ counter,
+                                                     double *__restrict__ out) {
+    __shared__ RedSmem<KP> sm;
+    double acc[KP] = {0.0};
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        double v = x[i];
+        acc[0] += squares ? v * v : v;
+    }
+    if (grid_reduce<KP>(acc, 1, partials, counter, sm) && threadIdx.x == 0)
+        out[0] = squares ? sqrt(sm.final_[0]) : sm.final_[0];
+}
+
+__global__ void k_fill(int64_t n, double *__restrict__ x, double v) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) x[i] = v;
+}
+
+__global__ void k_scale(int64_t n, double *__restrict__ x, const double *__restrict__ d_alpha, double alpha) {
+    const double a = alpha * (d_alpha ? d_alpha[0] : 1.0);
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) x[i] *= a;
+}
+
+static int max_stream_ctas() { return device_info().sm_count * 4; }
+
+cufsp_status launch_sum(int64_t n, const double *x, double *d_out, ReduceScratch &rs, cudaStream_t st) {
+    int g = stream_grid(n, 4, std::min(max_stream_ctas(), rs.max_ctas));
+    k_sum<1><<<g, kRedThreads, 0, st>>>(n, x, false, rs.partials, rs.counter, d_out);
+    CUFSP_CUDA_TRY(cudaGetLastError());
+    return CUFSP_SUCCESS;
+}
+
+cufsp_status launch_nrm2(int64_t n, const double *x, double *d_out, ReduceScratch &rs, cudaStream_t st) {
+    int g = stream_grid(n, 4, std::min(max_stream_ctas(), rs.max_ctas));
+    k_sum<1><<<g, kRedThreads, 0, st>>>(n, x, true, rs.partials, rs.counter, d_out);
+    CUFSP_CUDA_TRY(cudaGetLastError());
+    return CUFSP_SUCCESS;
+}
+
+cufsp_status launch_fill(int64_t n, double *x, double v, cudaStream_t st) {
+    int g = stream_grid(n, 4, max_stream_ctas());
+    k_fill<<<g, 256, 0, st>>>(n, x, v);
+    CUFSP_CUDA_TRY(cudaGetLastError());
+    return CUFSP_SUCCESS;
+}
+
+cufsp_status launch_scale(int64_t n, double *x, const double *d_alpha, double alpha, cudaStream_t st) {
+    int g = stream_grid(n, 4, max_stream_ctas());
+    k_scale<<<g, 256, 0, st>>>(n, x, d_alpha, alpha);
+    CUFSP_CUDA_TRY(cudaGetLastError());
+    return CUFSP_SUCCESS;
+}
+
+// ---- model validation -------------------------------------------------------------------------
+
+cufsp_status model_from_desc(const cufsp_model_desc *d, bool need_tables, ModelHost &m) {
+    if (!d) return set_error(CUFSP_ERR_INVALID_ARG, "model descriptor is NULL");
+    if (d->n_species < 1 || d->n_species > CUFSP_MAX_SPECIES)
+        return set_error(CUFSP_ERR_INVALID_ARG, "n_species must be in [1, 16]");
+    if (d->n_reactions < 1 || d->n_reactions > CUFSP_MAX_REACTIONS_SPARSE)
+        return set_error(CUFSP_ERR_INVALID_ARG, "n_reactions must be in [1, 256]");
+    if (!d->fsp_bounds || !d->stoich_vals || !d->stoich_colidxs || !d->stoich_rowptrs)
+        return set_error(CUFSP_ERR_INVALID_ARG, "fsp_bounds and the stoichiometry CSR arrays are required");
+    m.ns = d->n_species;
+    m.nr = d->n_reactions;
+    m.bounds.assign(d->fsp_bounds, d->fsp_bounds + m.ns);
+    int64_t n = 1;
+    for (int s = 0; s < m.ns; ++s) {
+        if (m.bounds[s] < 0) return set_error(CUFSP_ERR_INVALID_ARG, "fsp_bounds must be >= 0");
+        n *= (int64_t)m.bounds[s] + 1;
+        if (n > 2147483647LL)
+            return set_error(CUFSP_ERR_OVERFLOW, "number of states exceeds 2^31-1 (int32 state index)");
+    }
+    m.n = n;
+    m.nu.assign((size_t)m.nr * m.ns, 0);
+    if (d->stoich_rowptrs[0] != 0) return set_error(CUFSP_ERR_INVALID_ARG, "stoich_rowptrs[0] must be 0");
+    for (int r = 0; r < m.nr; ++r) {
+        int a = d->stoich_rowptrs[r], b = d->stoich_rowptrs[r + 1];
+        if (b < a) return set_error(CUFSP_ERR_INVALID_ARG, "stoich_rowptrs must be non-decreasing");
+        for (int i = a; i < b; ++i) {
+            int c = d->stoich_colidxs[i];
+            if (c < 0 || c >= m.ns) return set_error(CUFSP_ERR_INVALID_ARG, "stoich column index out of range");
+            m.nu[(size_t)r * m.ns + c] += d->stoich_vals[i];
+        }
+    }
+    m.tab_off.resize(m.ns);
+    int off = 0;
+    for (int s = 0; s < m.ns; ++s) {
+        m.tab_off[s] = off;
+        off += m.bounds[s] + 1;
+    }
+    m.tab_stride = off;
+    m.prop_device = d->prop_device;
+    m.tcoef = d->tcoef;
+    m.tcoef_user = d->tcoef_user;
+    const size_t tsz = (size_t)m.nr * m.tab_stride;
+    if (d->factor_tables) {
+        m.tables.assign(d->factor_tables, d->factor_tables + tsz);
+    } else if (d->prop_factor) {
+        // fspmat_sdkron_fill_host_data (src/fspmat_kron_kernels.cu:170-190): f_{r,s}(0..b_s)
+        m.tables.resize(tsz);
+        size_t iv = 0;
+        for (int r = 0; r < m.nr; ++r)
+            for (int s = 0; s < m.ns; ++s)
+                for (int x = 0; x <= m.bounds[s]; ++x) m.tables[iv++] = d->prop_factor(x, s, r);
+    }
+    for (double v : m.tables)
+        if (!std::isfinite(v)) return set_error(CUFSP_ERR_NONFINITE, "propensity factor table holds NaN/Inf");
+    if (need_tables && m.tables.empty())
+        return set_error(CUFSP_ERR_INVALID_ARG, "KRONECKER format needs factor_tables or prop_factor");
+    if (m.tables.empty() && !m.prop_device)
+        return set_error(CUFSP_ERR_INVALID_ARG, "no propensity source (factor_tables, prop_factor or prop_device)");
+    return CUFSP_SUCCESS;
+}
+
+}  // namespace cufsp
+
+using namespace cufsp;
+
+// ---- C ABI: status and indexing --------------------------------------------------------------
+
+extern "C" const char *cufsp_status_string(cufsp_status s) {
+    switch (s) {
+        case CUFSP_SUCCESS: return "CUFSP_SUCCESS";
+        case CUFSP_ERR_INVALID_ARG: return "CUFSP_ERR_INVALID_ARG";
+        case CUFSP_ERR_OVERFLOW: return "CUFSP_ERR_OVERFLOW";
+        case CUFSP_ERR_ALLOC: return "CUFSP_ERR_ALLOC";
+        case CUFSP_ERR_CUDA: return "CUFSP_ERR_CUDA";
+        case CUFSP_ERR_NONFINITE: return "CUFSP_ERR_NONFINITE";
+        case CUFSP_ERR_STEP_LIMIT: return "CUFSP_ERR_STEP_LIMIT";
+        case CUFSP_ERR_UNSUPPORTED: return "CUFSP_ERR_UNSUPPORTED";
+        case CUFSP_ERR_NO_DEVICE: return "CUFSP_ERR_NO_DEVICE";
+    }
+    return "CUFSP_ERR_UNKNOWN";
+}
+
+extern "C" const char *cufsp_last_error(void) { return g_last_error.c_str(); }
+
+extern "C" cufsp_status cufsp_num_states(int ns, const int *bounds, int64_t *n_states) {
+    if (!bounds || !n_states || ns < 1) return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_num_states: bad argument");
+    int64_t n = 1;
+    for (int s = 0; s < ns; ++s) {
+        if (bounds[s] < 0) return set_error(CUFSP_ERR_INVALID_ARG, "fsp_bounds must be >= 0");
+        n *= (int64_t)bounds[s] + 1;
+        if (n > ((int64_t)1 << 62)) return set_error(CUFSP_ERR_OVERFLOW, "state count overflow");
+    }
+    *n_states = n;
+    return CUFSP_SUCCESS;
+}
+
+extern "C" cufsp_status cufsp_indx2state(int64_t indx, int *state, int ns, const int *bounds) {
+    if (!state || !bounds || ns < 1 || indx < 0) return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_indx2state: bad argument");
+    for (int s = 0; s < ns; ++s) {
+        int64_t d = (int64_t)bounds[s] + 1;
+        state[s] = (int)(indx % d);
+        indx /= d;
+    }
+    return CUFSP_SUCCESS;
+}
+
+extern "C" cufsp_status cufsp_state2indx(const int *state, int ns, const int *bounds, int64_t *indx) {
+    if (!state || !bounds || !indx || ns < 1) return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_state2indx: bad argument");
+    int64_t id = 0, np = 1;
+    for (int s = 0; s < ns; ++s) {
+        if (state[s] < 0 || state[s] > bounds[s]) return set_error(CUFSP_ERR_INVALID_ARG, "state outside the FSP box");
+        id += (int64_t)state[s] * np;
+        np *= (int64_t)bounds[s] + 1;
+    }
+    *indx = id;
+    return CUFSP_SUCCESS;
+}
+
+extern "C" cufsp_status cufsp_get_states(int ns, const int *bounds, int *d_states, cufsp_stream_t stream) {
+    if (!bounds || !d_states || ns < 1 || ns > CUFSP_MAX_SPECIES)
+        return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_get_states: bad argument");
+    int64_t n = 0;
+    cufsp_status s = cufsp_num_states(ns, bounds, &n);
+    if (s != CUFSP_SUCCESS) return s;
+    if (n > 2147483647LL) return set_error(CUFSP_ERR_OVERFLOW, "number of states exceeds 2^31-1");
+    DecodeArgs a;
+    a.ns = ns;
+    for (int k = 0; k < ns; ++k) a.div[k] = make_fastdiv((uint32_t)bounds[k] + 1u);
+    int64_t grid = (n + 255) / 256;
+    k_get_states<<<(unsigned)grid, 256, 256 * ns * sizeof(int), (cudaStream_t)stream>>>(a, (int)n, d_states);
+    CUFSP_CUDA_TRY(cudaGetLastError());
+    return CUFSP_SUCCESS;
+}
+
+extern "C" cufsp_status cufsp_vec_sum(int64_t n, const double *x, double *out, cufsp_stream_t stream) {
+    if (!x || !out || n < 0) return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_vec_sum: bad argument");
+    ReduceScratch rs;
+    cufsp_status s = rs.init(device_info().sm_count * 4, 1);
+    if (s != CUFSP_SUCCESS) { rs.release(); return s; }
+    double *d_out = nullptr;
+    if (cudaMalloc(&d_out, sizeof(double)) != cudaSuccess) { rs.release(); return set_error(CUFSP_ERR_ALLOC, "cudaMalloc"); }
+    s = launch_sum(n, x, d_out, rs, (cudaStream_t)stream);
+    if (s == CUFSP_SUCCESS) {
+        cudaError_t e = cudaMemcpyAsync(out, d_out, sizeof(double), cudaMemcpyDeviceToHost, (cudaStream_t)stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize((cudaStream_t)stream);
+        if (e != cudaSuccess) s = cuda_error(e, "cufsp_vec_sum");
+    }
+    cudaFree(d_out);
+    rs.release();
+    return s;
+}

@@ -1,0 +1,141 @@
+// cufsp_internal.h -- shared declarations of the cufsp CUDA library (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/cufsp.h"
+
+#define CUFSP_MAX_SPECIES 16
+#define CUFSP_MAX_REACTIONS 32   // KRONECKER register path; the sparse path allows CUFSP_MAX_REACTIONS_SPARSE
+#define CUFSP_MAX_REACTIONS_SPARSE 256
+#define CUFSP_MAX_KRYLOV 60  // m + 1 basis vectors must fit the 64-wide multi-vector kernels
+
+namespace cufsp {
+
+// Thread-local last-error text; set_error returns the status for `return set_error(...)`.
+cufsp_status set_error(cufsp_status s, const std::string &msg);
+cufsp_status cuda_error(cudaError_t e, const char *what);
+void clear_error();
+
+#define CUFSP_CUDA_TRY(call)                                              \
+    do {                                                                  \
+        cudaError_t _e = (call);                                          \
+        if (_e != cudaSuccess) return ::cufsp::cuda_error(_e, #call);     \
+    } while (0)
+
+// Device properties cached per device id.
+struct DeviceInfo {
+    int sm_count = 0;
+    int max_smem_optin = 0;
+};
+const DeviceInfo &device_info();
+
+// Fast unsigned division by a runtime constant for numerators < 2^31
+// (round-up multiplier method of Granlund & Montgomery, PLDI 1994):
+//   l = ceil(log2 d), M = floor(2^32 (2^l - d) / d) + 1, q = (umulhi(M, n) + n) >> l.
+struct FastDiv {
+    uint32_t d;
+    uint32_t mul;
+    uint32_t shift;
+};
+FastDiv make_fastdiv(uint32_t d);
+
+#if defined(__CUDACC__)
+__host__ __device__ __forceinline__ uint32_t fd_div(uint32_t n, const FastDiv &f) {
+#if defined(__CUDA_ARCH__)
+    uint32_t t = __umulhi(n, f.mul);
+#else
+    uint32_t t = (uint32_t)(((uint64_t)n * f.mul) >> 32);
+#endif
+    return (t + n) >> f.shift;
+}
+#endif
+
+// Reduction scratch shared by the vector kernels of one handle: per-CTA partials and a
+// completion counter for the last-CTA-reduces pattern (deterministic summation order).
+struct ReduceScratch {
+    double *partials = nullptr;  // [max_ctas * max_k]
+    unsigned int *counter = nullptr;
+    int max_ctas = 0;
+    int max_k = 0;
+    cufsp_status init(int max_ctas, int max_k);
+    void release();
+};
+
+// Grid for a streaming vector kernel of n elements with 256 threads per CTA.
+int stream_grid(int64_t n, int elems_per_thread, int max_ctas);
+
+// sum / dot / norm primitives (cufsp_common.cu)
+cufsp_status launch_sum(int64_t n, const double *x, double *d_out, ReduceScratch &rs, cudaStream_t st);
+cufsp_status launch_nrm2(int64_t n, const double *x, double *d_out, ReduceScratch &rs, cudaStream_t st);
+cufsp_status launch_fill(int64_t n, double *x, double v, cudaStream_t st);
+cufsp_status launch_scale(int64_t n, double *x, const double *d_alpha, double alpha, cudaStream_t st);
+
+// Model data validated and normalised on the host.
+struct ModelHost {
+    int ns = 0, nr = 0;
+    int64_t n = 0;
+    std::vector<int> bounds;       // b_s
+    std::vector<int> nu;           // dense stoichiometry [nr][ns]
+    std::vector<double> tables;    // [nr][sum_s(b_s+1)] or empty
+    std::vector<int> tab_off;      // [ns] offset of species s inside a reaction's block
+    int tab_stride = 0;            // sum_s (b_s + 1)
+    cufsp_prop_fn prop_device = nullptr;
+    cufsp_tcoef_fn tcoef = nullptr;
+    void *tcoef_user = nullptr;
+};
+cufsp_status model_from_desc(const cufsp_model_desc *d, bool need_tables, ModelHost &m);
+
+// ---- format back-ends ----------------------------------------------------------------------
+struct KronData;    // matrix-free factorised generator (cufsp_kron.cu)
+struct SparseData;  // reaction-major propensity table (cufsp_sparse.cu)
+
+cufsp_status kron_create(const ModelHost &m, KronData **out);
+void kron_destroy(KronData *k);
+// y = alpha * A(coefs) x (+ y if accumulate); d_alpha (nullable) multiplies alpha on the device;
+// the kernel returns at once when d_skip is non-null and *d_skip != 0.
+// Rows [q_begin, q_end) of the outer index only (q_end < 0: all rows).
+cufsp_status kron_apply(KronData *k, const double *coefs, double alpha, const double *d_alpha,
+                        const int *d_skip, const double *x, bool accumulate, double *y, cudaStream_t st,
+                        int64_t i_begin = 0, int64_t i_end = -1);
+// halo (max |shift|) and slab granularity for the host-buffer pipeline
+int64_t kron_halo(const KronData *k);
+int64_t kron_row_len(const KronData *k);
+
+cufsp_status sparse_create(const ModelHost &m, SparseData **out);
+void sparse_destroy(SparseData *s);
+cufsp_status sparse_apply(SparseData *s, const double *coefs, double alpha, const double *d_alpha,
+                          const int *d_skip, const double *x, bool accumulate, double *y, cudaStream_t st,
+                          int64_t i_begin = 0, int64_t i_end = -1);
+cufsp_status sparse_export(const SparseData *s, double *d_props, cudaStream_t st);
+int64_t sparse_halo(const SparseData *s);
+
+// Host-side dense exponential (cufsp_expm.cpp).
+cufsp_status expm_pade13(int k, const double *A, double *F);
+
+}  // namespace cufsp
+
+// Opaque handle behind cufsp_mat.
+struct cufsp_mat_s {
+    cufsp::ModelHost model;
+    cufsp_format format = CUFSP_FORMAT_KRONECKER;
+    cufsp::KronData *kron = nullptr;
+    cufsp::SparseData *sparse = nullptr;
+    std::vector<double> coef_buf;
+    // host-buffer pipeline resources (created on first use)
+    double *d_x = nullptr, *d_y = nullptr;
+    cudaStream_t s_in = nullptr, s_comp = nullptr, s_out = nullptr;
+    std::vector<cudaEvent_t> ev;
+};
+
+namespace cufsp {
+// d_skip (nullable): the kernels return at once when *d_skip != 0 (Krylov breakdown / error flag).
+cufsp_status mat_apply(cufsp_mat *A, const double *coefs, double alpha, const double *d_alpha, const int *d_skip,
+                       const double *x, bool accumulate, double *y, cudaStream_t st, int64_t i_begin = 0,
+                       int64_t i_end = -1);
+cufsp_status mat_coefs(cufsp_mat *A, double t, const double *coefs_in, std::vector<double> &out);
+}  // namespace cufsp

@@ -1,0 +1,515 @@
+// cufsp_krylov.cu -- adaptive Krylov exp(tA)v (replaces cuFSP::KryExpvFSP,
+// src/KryExpvFSP.h:20-108, src/KryExpvFSP.cu:6-203).
+//
+// Same algorithm as the reference (Expokit expv step control, classical Gram-Schmidt Arnoldi with
+// optional incomplete orthogonalisation, augmented (m+2)x(m+2) Hessenberg matrix, phi1/phi2 error
+// estimate), re-organised so that a whole Arnoldi pass runs on the device without host round trips:
+//  * basis vectors are stored as W_k with v_k = rho_k W_k (rho on the device): the generator kernel
+//    scales its output by rho_j read from device memory, and the normalisation pass of the reference
+//    (cublasDscal, KryExpvFSP.cu:103-105) disappears;
+//  * h = V^T w is one multi-vector dot kernel (each element of w read once for all j+1 dots), and
+//    w -= V h is fused with the norm ||w|| (KryExpvFSP.cu:76-86 did gemv T, gemv N, nrm2);
+//  * reductions finish in the last CTA (deterministic order) which also writes H(:, j), H(j+1, j),
+//    rho_{j+1} and the happy-breakdown flag; kernels after a breakdown return at once;
+//  * W_0 is the caller's vector itself (the reference copied it into the workspace, :60-64): the
+//    final combination v = beta V F(:,0) (:165-166) reads each W_k[i] before writing v[i].
+// One device->host copy of (H, rho, beta, flags) per step feeds the host step control, where the
+// (m+2)^2 exponential is taken (Pade(13,13)).
+// Deviations from the reference: k1 is reset every step (reference defect: KryExpvFSP.h:61), pi is
+// exact (:48), a zero vector is returned unchanged, NaN/Inf and exhausted limits return errors.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "cufsp_internal.h"
+#include "cufsp_reduce.cuh"
+
+namespace cufsp {
+
+constexpr int kMaxVec = CUFSP_MAX_KRYLOV + 1;
+
+// Device state block (doubles, then one int flag):
+//   H[(m+2)^2] | rho[m+2] | gam[m+2] | beta | avnorm | pad | pad | flag(int)
+struct KState {
+    double *H, *rho, *gam, *beta, *avnorm;
+    int *flag;  // 0 ok, >0 happy breakdown at mb = flag, -1 NaN/Inf, -2 zero vector
+    int mp2;
+};
+
+__global__ void __launch_bounds__(kRedThreads) k_step_begin(int64_t n, const double *__restrict__ v, KState s,
+                                                            double *__restrict__ partials,
+                                                            unsigned int *__restrict__ counter) {
+    __shared__ RedSmem<1> sm;
+    double acc[1] = {0.0};
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const double t = v[i];
+        acc[0] = fma(t, t, acc[0]);
+    }
+    if (!grid_reduce<1>(acc, 1, partials, counter, sm)) return;
+    const double beta = sqrt(sm.final_[0]);
+    for (int i = threadIdx.x; i < s.mp2 * s.mp2; i += blockDim.x) s.H[i] = 0.0;
+    for (int i = threadIdx.x; i < s.mp2; i += blockDim.x) {
+        s.rho[i] = 0.0;
+        s.gam[i] = 0.0;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        *s.beta = beta;
+        *s.avnorm = 0.0;
+        s.rho[0] = (beta > 0.0) ? 1.0 / beta : 0.0;
+        *s.flag = !isfinite(beta) ? -1 : (beta == 0.0 ? -2 : 0);
+    }
+}
+
+struct MVecArgs {
+    const double *vec[kMaxVec];
+    double *w;
+    int64_t n;
+    int K;      // number of basis vectors used (istart..j)
+    int kbase;  // istart
+    int j;
+    double btol;
+    KState s;
+    double *partials;
+    unsigned int *counter;
+};
+
+// h_k = rho_k * (W_k . W_{j+1}) for k = istart..j;  H(k, j) = h_k;  gam_k = h_k * rho_k.
+template <int KP>
+__global__ void __launch_bounds__(kRedThreads) k_mdot(const MVecArgs a) {
+    __shared__ RedSmem<KP> sm;
+    if (*a.s.flag) return;
+    double acc[KP];
+#pragma unroll
+    for (int k = 0; k < KP; ++k) acc[k] = 0.0;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride) {
+        const double wi = a.w[i];
+#pragma unroll
+        for (int k = 0; k < KP; ++k)
+            if (k < a.K) acc[k] = fma(__ldg(a.vec[k] + i), wi, acc[k]);
+    }
+    if (!grid_reduce<KP>(acc, a.K, a.partials, a.counter, sm)) return;
+    for (int k = threadIdx.x; k < a.K; k += blockDim.x) {
+        const int kk = a.kbase + k;
+        const double r = a.s.rho[kk];
+        const double h = r * sm.final_[k];
+        a.s.H[kk + a.j * a.s.mp2] = h;
+        a.s.gam[kk] = h * r;
+    }
+}
+
+// W_{j+1} -= sum_k gam_k W_k;  s = rho_j-scaled norm;  H(j+1, j) = s;  rho_{j+1} = 1/s;
+// happy breakdown when s < btol (src/KryExpvFSP.cu:76-105).
+template <int KP>
+__global__ void __launch_bounds__(kRedThreads) k_mupd(const MVecArgs a) {
+    __shared__ RedSmem<1> sm;
+    __shared__ double g[KP];
+    if (*a.s.flag) return;
+    for (int k = threadIdx.x; k < KP; k += blockDim.x) g[k] = (k < a.K) ? a.s.gam[a.kbase + k] : 0.0;
+    __syncthreads();
+    double acc[1] = {0.0};
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride) {
+        double wi = a.w[i];
+#pragma unroll
+        for (int k = 0; k < KP; ++k)
+            if (k < a.K) wi = fma(-g[k], __ldg(a.vec[k] + i), wi);
+        a.w[i] = wi;
+        acc[0] = fma(wi, wi, acc[0]);
+    }
+    if (!grid_reduce<1>(acc, 1, a.partials, a.counter, sm)) return;
+    if (threadIdx.x == 0) {
+        const double sn = sqrt(sm.final_[0]);
+        if (!isfinite(sn)) {
+            *a.s.flag = -1;
+        } else if (sn < a.btol) {
+            *a.s.flag = a.j + 1;
+        } else {
+            a.s.H[(a.j + 1) + a.j * a.s.mp2] = sn;
+            a.s.rho[a.j + 1] = 1.0 / sn;
+        }
+    }
+}
+
+// avnorm = ||A v_m|| (src/KryExpvFSP.cu:114-120); skipped after a breakdown.
+__global__ void __launch_bounds__(kRedThreads) k_avnorm(int64_t n, const double *__restrict__ w, KState s,
+                                                        double *__restrict__ partials,
+                                                        unsigned int *__restrict__ counter) {
+    __shared__ RedSmem<1> sm;
+    if (*s.flag) return;
+    double acc[1] = {0.0};
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const double t = w[i];
+        acc[0] = fma(t, t, acc[0]);
+    }
+    if (grid_reduce<1>(acc, 1, partials, counter, sm) && threadIdx.x == 0) {
+        const double av = sqrt(sm.final_[0]);
+        *s.avnorm = av;
+        if (!isfinite(av)) *s.flag = -1;
+    }
+}
+
+struct CombArgs {
+    const double *vec[kMaxVec];
+    double *out;  // may alias vec[0]
+    int64_t n;
+    int K;
+    double c[kMaxVec];
+};
+
+// out = sum_k c_k W_k  (sol = beta V F(:,0), src/KryExpvFSP.cu:160-166).
+template <int KP>
+__global__ void __launch_bounds__(256) k_comb(const CombArgs a) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride) {
+        double acc = 0.0;
+#pragma unroll
+        for (int k = 0; k < KP; ++k)
+            if (k < a.K) acc = fma(a.c[k], a.vec[k][i], acc);
+        a.out[i] = acc;
+    }
+}
+
+}  // namespace cufsp
+
+using namespace cufsp;
+
+struct cufsp_expv_s {
+    int64_t n = 0;
+    int m = 30;
+    double tol = 1e-8;
+    int iop = 0, q_iop = 2;
+    double anorm = 1.0;
+    int64_t max_nstep = 10000, max_reject = 1000;
+    double t_final = 0.0, t_now = 0.0, t_new = 0.0, btol = 0.0, xm = 0.0;
+    int64_t i_step = 0;
+    cufsp_mat *A = nullptr;
+    std::vector<double> coefs;
+    cufsp_matvec_fn fn = nullptr;
+    void *user = nullptr;
+    double *W = nullptr;       // W_1 .. W_{m+1}
+    double *d_state = nullptr; // KState block
+    KState ks;
+    size_t state_bytes = 0;
+    ReduceScratch rs;
+    int grid = 1;
+    std::vector<double> hstate, Hh, F, tH;
+    cufsp_expv_stats stats;
+};
+
+namespace {
+
+inline double *wvec(cufsp_expv *E, double *v, int k) { return k == 0 ? v : E->W + (size_t)(k - 1) * E->n; }
+
+cufsp_status matvec(cufsp_expv *E, const double *x, double *y, const double *d_alpha, cudaStream_t st) {
+    if (E->A) return mat_apply(E->A, E->coefs.data(), 1.0, d_alpha, E->ks.flag, x, false, y, st);
+    // MVFun form (src/KryExpvFSP.h:15): the callback accumulates into a zeroed y.
+    cufsp_status s = launch_fill(E->n, y, 0.0, st);
+    if (s != CUFSP_SUCCESS) return s;
+    if (E->fn(x, y, E->user, (cufsp_stream_t)st) != 0)
+        return set_error(CUFSP_ERR_INVALID_ARG, "expv: matvec callback returned an error");
+    return launch_scale(E->n, y, d_alpha, 1.0, st);
+}
+
+template <int KP>
+void launch_mdot(const MVecArgs &a, int grid, cudaStream_t st) { k_mdot<KP><<<grid, kRedThreads, 0, st>>>(a); }
+template <int KP>
+void launch_mupd(const MVecArgs &a, int grid, cudaStream_t st) { k_mupd<KP><<<grid, kRedThreads, 0, st>>>(a); }
+template <int KP>
+void launch_comb(const CombArgs &a, int grid, cudaStream_t st) { k_comb<KP><<<grid, 256, 0, st>>>(a); }
+
+cufsp_status arnoldi_dot_update(cufsp_expv *E, double *v, int j, int istart, cudaStream_t st) {
+    MVecArgs a;
+    a.K = j - istart + 1;
+    a.kbase = istart;
+    for (int k = 0; k < a.K; ++k) a.vec[k] = wvec(E, v, istart + k);
+    a.w = wvec(E, v, j + 1);
+    a.n = E->n;
+    a.j = j;
+    a.btol = E->btol;
+    a.s = E->ks;
+    a.partials = E->rs.partials;
+    a.counter = E->rs.counter;
+    const int K = a.K;
+    if (K <= 8) launch_mdot<8>(a, E->grid, st);
+    else if (K <= 16) launch_mdot<16>(a, E->grid, st);
+    else if (K <= 32) launch_mdot<32>(a, E->grid, st);
+    else launch_mdot<64>(a, E->grid, st);
+    CUFSP_CUDA_TRY(cudaGetLastError());
+    if (K <= 8) launch_mupd<8>(a, E->grid, st);
+    else if (K <= 16) launch_mupd<16>(a, E->grid, st);
+    else if (K <= 32) launch_mupd<32>(a, E->grid, st);
+    else launch_mupd<64>(a, E->grid, st);
+    CUFSP_CUDA_TRY(cudaGetLastError());
+    return CUFSP_SUCCESS;
+}
+
+double round2(double t) {
+    const double s = std::pow(10.0, std::floor(std::log10(t)) - 1.0);
+    return std::ceil(t / s) * s;
+}
+
+cufsp_status expv_step(cufsp_expv *E, double *v, cudaStream_t st) {
+    if (!E->A && !E->fn) return set_error(CUFSP_ERR_INVALID_ARG, "expv: no operator bound");
+    if (E->t_now >= E->t_final) return CUFSP_SUCCESS;
+    if (E->i_step >= E->max_nstep) return set_error(CUFSP_ERR_STEP_LIMIT, "expv: max_nstep reached");
+    const int m = E->m, mp2 = m + 2;
+    const double delta = 1.2, gamma = 0.9;
+    if (E->i_step == 0) E->btol = E->anorm * E->tol;  // tolerance for happy breakdown (:50)
+
+    // ---- Arnoldi pass, entirely on the device ----
+    k_step_begin<<<E->grid, kRedThreads, 0, st>>>(E->n, v, E->ks, E->rs.partials, E->rs.counter);
+    CUFSP_CUDA_TRY(cudaGetLastError());
+    cufsp_status s;
+    int istart = 0;
+    for (int j = 0; j < m; ++j) {
+        s = matvec(E, wvec(E, v, j), wvec(E, v, j + 1), E->ks.rho + j, st);
+        if (s != CUFSP_SUCCESS) return s;
+        if (E->iop) istart = (j >= E->q_iop - 1) ? j - E->q_iop + 1 : 0;
+        s = arnoldi_dot_update(E, v, j, istart, st);
+        if (s != CUFSP_SUCCESS) return s;
+    }
+    s = matvec(E, wvec(E, v, m), wvec(E, v, m + 1), E->ks.rho + m, st);
+    if (s != CUFSP_SUCCESS) return s;
+    k_avnorm<<<E->grid, kRedThreads, 0, st>>>(E->n, wvec(E, v, m + 1), E->ks, E->rs.partials, E->rs.counter);
+    CUFSP_CUDA_TRY(cudaGetLastError());
+    CUFSP_CUDA_TRY(cudaMemcpyAsync(E->hstate.data(), E->d_state, E->state_bytes, cudaMemcpyDeviceToHost, st));
+    CUFSP_CUDA_TRY(cudaStreamSynchronize(st));
+
+    const double *hH = E->hstate.data();
+    const double *hrho = hH + (size_t)mp2 * mp2;
+    const double beta = hrho[2 * mp2];
+    const double avnorm = hrho[2 * mp2 + 1];
+    int flag;
+    std::memcpy(&flag, hrho + 2 * mp2 + 4, sizeof(int));
+    if (flag == -2) {  // zero vector: exp(tA) 0 = 0
+        E->t_now = E->t_final;
+        return CUFSP_SUCCESS;
+    }
+    if (flag == -1) return set_error(CUFSP_ERR_NONFINITE, "expv: NaN/Inf in the Krylov iteration");
+
+    if (E->i_step == 0) {  // first-step size, src/KryExpvFSP.cu:45-51
+        E->xm = 1.0 / (double)m;
+        const double fact = std::pow((m + 1) / std::exp(1.0), m + 1) * std::sqrt(2.0 * M_PI * (m + 1));
+        E->t_new = (1.0 / E->anorm) * std::pow((fact * E->tol) / (4.0 * beta * E->anorm), E->xm);
+    }
+    int mb = m, k1 = 2;
+    double tau = std::min(E->t_final - E->t_now, E->t_new);
+    int64_t n_mv = m + 1;
+    if (flag > 0) {  // happy breakdown (:90-98)
+        k1 = 0;
+        mb = flag;
+        tau = E->t_final - E->t_now;
+        n_mv = mb;
+        E->stats.n_breakdown++;
+    }
+    E->stats.n_matvec += n_mv;
+    std::memcpy(E->Hh.data(), hH, sizeof(double) * mp2 * mp2);
+    if (k1 != 0) E->Hh[(m + 1) + (size_t)m * mp2] = 1.0;
+
+    double err_loc = 0.0;
+    int64_t ireject = 0;
+    bool accepted = false;
+    while (ireject < E->max_reject) {  // rejection loop, :122-158
+        const int mx = mb + k1;
+        for (int i = 0; i < mp2 * mp2; ++i) E->tH[i] = tau * E->Hh[i];
+        s = expm_pade13(mp2, E->tH.data(), E->F.data());
+        if (s != CUFSP_SUCCESS) return s;
+        if (k1 == 0) {
+            err_loc = E->btol;
+            accepted = true;
+            break;
+        }
+        const double phi1 = std::fabs(beta * E->F[mx - 2]);
+        const double phi2 = std::fabs(beta * E->F[mx - 1] * avnorm);
+        if (phi1 > phi2 * 10.0) {
+            err_loc = phi2;
+            E->xm = 1.0 / (double)mx;
+        } else if (phi1 > phi2) {
+            err_loc = (phi1 * phi2) / (phi1 - phi2);
+            E->xm = 1.0 / (double)mx;
+        } else {
+            err_loc = phi1;
+            E->xm = 1.0 / (double)(mx - 1);
+        }
+        if (!std::isfinite(err_loc)) return set_error(CUFSP_ERR_NONFINITE, "expv: non-finite error estimate");
+        if (err_loc <= delta * tau * E->tol) {
+            accepted = true;
+            break;
+        }
+        tau = round2(gamma * tau * std::pow(tau * E->tol / err_loc, E->xm));
+        ++ireject;
+        E->stats.n_reject++;
+    }
+    if (!accepted) return set_error(CUFSP_ERR_STEP_LIMIT, "expv: max_reject reached");
+
+    // v = beta * V[:, 0:mx] F(0:mx, 0) = sum_k (beta F_k0 rho_k) W_k
+    const int mx = mb + std::max(0, k1 - 1);
+    CombArgs c;
+    c.K = mx;
+    c.n = E->n;
+    c.out = v;
+    for (int k = 0; k < mx; ++k) {
+        c.vec[k] = wvec(E, v, k);
+        c.c[k] = beta * E->F[k] * hrho[k];
+    }
+    const int g = stream_grid(E->n, 4, device_info().sm_count * 8);
+    if (mx <= 8) launch_comb<8>(c, g, st);
+    else if (mx <= 16) launch_comb<16>(c, g, st);
+    else if (mx <= 32) launch_comb<32>(c, g, st);
+    else launch_comb<64>(c, g, st);
+    CUFSP_CUDA_TRY(cudaGetLastError());
+
+    const bool last = (tau >= E->t_final - E->t_now);
+    E->t_now = last ? E->t_final : E->t_now + tau;
+    if (err_loc > 0.0) E->t_new = round2(gamma * tau * std::pow(tau * E->tol / err_loc, E->xm));
+    if (!(E->t_new > 0.0) || !std::isfinite(E->t_new)) E->t_new = E->t_final - E->t_now;
+    E->i_step++;
+    E->stats.n_steps++;
+    E->stats.t_now = E->t_now;
+    E->stats.last_err = err_loc;
+    return CUFSP_SUCCESS;
+}
+
+}  // namespace
+
+extern "C" cufsp_status cufsp_expv_create(int64_t n, int m, double tol, int iop, int q_iop, double anorm,
+                                          cufsp_expv **out) {
+    clear_error();
+    if (!out) return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_expv_create: out is NULL");
+    *out = nullptr;
+    if (n < 1 || n > 2147483647LL) return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_expv_create: n out of range");
+    if (m < 1 || m > CUFSP_MAX_KRYLOV) return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_expv_create: m must be in [1, 60]");
+    if (!(tol > 0.0) || !(anorm > 0.0)) return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_expv_create: tol and anorm must be > 0");
+    if (iop && q_iop < 1) return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_expv_create: q_iop must be >= 1");
+    cufsp_expv *E = new cufsp_expv();
+    E->n = n;
+    E->m = m;
+    E->tol = tol;
+    E->iop = iop;
+    E->q_iop = q_iop;
+    E->anorm = anorm;
+    const int mp2 = m + 2;
+    const size_t nd = (size_t)mp2 * mp2 + 2 * (size_t)mp2 + 4;
+    E->state_bytes = nd * sizeof(double) + 2 * sizeof(int);
+    E->hstate.resize(nd + 1);
+    E->Hh.resize((size_t)mp2 * mp2);
+    E->F.resize((size_t)mp2 * mp2);
+    E->tH.resize((size_t)mp2 * mp2);
+    std::memset(&E->stats, 0, sizeof(E->stats));
+    cudaError_t e = cudaMalloc(&E->W, sizeof(double) * (size_t)n * (size_t)(m + 1));
+    if (e == cudaSuccess) e = cudaMalloc(&E->d_state, E->state_bytes);
+    if (e == cudaSuccess) e = cudaMemset(E->d_state, 0, E->state_bytes);
+    if (e != cudaSuccess) {
+        cufsp_expv_destroy(E);
+        return cuda_error(e, "cufsp_expv_create");
+    }
+    double *b = E->d_state;
+    E->ks.H = b;
+    E->ks.rho = b + (size_t)mp2 * mp2;
+    E->ks.gam = E->ks.rho + mp2;
+    E->ks.beta = E->ks.gam + mp2;
+    E->ks.avnorm = E->ks.beta + 1;
+    E->ks.flag = reinterpret_cast<int *>(E->ks.beta + 4);
+    E->ks.mp2 = mp2;
+    E->grid = stream_grid(n, 4, device_info().sm_count * 4);
+    cufsp_status s = E->rs.init(E->grid, 64);
+    if (s != CUFSP_SUCCESS) {
+        cufsp_expv_destroy(E);
+        return s;
+    }
+    *out = E;
+    return CUFSP_SUCCESS;
+}
+
+extern "C" cufsp_status cufsp_expv_destroy(cufsp_expv *E) {
+    if (!E) return CUFSP_SUCCESS;
+    if (E->W) cudaFree(E->W);
+    if (E->d_state) cudaFree(E->d_state);
+    E->rs.release();
+    delete E;
+    return CUFSP_SUCCESS;
+}
+
+extern "C" cufsp_status cufsp_expv_set_limits(cufsp_expv *E, int64_t max_nstep, int64_t max_reject) {
+    if (!E || max_nstep < 1 || max_reject < 1) return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_expv_set_limits: bad argument");
+    E->max_nstep = max_nstep;
+    E->max_reject = max_reject;
+    return CUFSP_SUCCESS;
+}
+
+extern "C" cufsp_status cufsp_expv_bind_mat_coefs(cufsp_expv *E, cufsp_mat *A, const double *coefs) {
+    if (!E || !A) return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_expv_bind_mat: NULL argument");
+    int64_t n = 0;
+    cufsp_mat_num_states(A, &n);
+    if (n != E->n) return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_expv_bind_mat: size mismatch");
+    cufsp_status s = mat_coefs(A, 0.0, coefs, E->coefs);
+    if (s != CUFSP_SUCCESS) return s;
+    E->A = A;
+    E->fn = nullptr;
+    return CUFSP_SUCCESS;
+}
+
+extern "C" cufsp_status cufsp_expv_bind_mat(cufsp_expv *E, cufsp_mat *A, double t_mat) {
+    if (!E || !A) return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_expv_bind_mat: NULL argument");
+    std::vector<double> c;
+    cufsp_status s = mat_coefs(A, t_mat, nullptr, c);
+    if (s != CUFSP_SUCCESS) return s;
+    return cufsp_expv_bind_mat_coefs(E, A, c.data());
+}
+
+extern "C" cufsp_status cufsp_expv_bind_matvec(cufsp_expv *E, cufsp_matvec_fn fn, void *user) {
+    if (!E || !fn) return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_expv_bind_matvec: NULL argument");
+    E->fn = fn;
+    E->user = user;
+    E->A = nullptr;
+    return CUFSP_SUCCESS;
+}
+
+extern "C" cufsp_status cufsp_expv_set_final_time(cufsp_expv *E, double t_final) {
+    if (!E || !(t_final >= 0.0) || !std::isfinite(t_final))
+        return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_expv_set_final_time: bad argument");
+    E->t_final = t_final;
+    return CUFSP_SUCCESS;
+}
+
+extern "C" cufsp_status cufsp_expv_step(cufsp_expv *E, double *v, cufsp_stream_t stream) {
+    if (!E || !v) return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_expv_step: NULL argument");
+    return expv_step(E, v, (cudaStream_t)stream);
+}
+
+extern "C" cufsp_status cufsp_expv_solve(cufsp_expv *E, double *v, cufsp_stream_t stream, cufsp_expv_stats *stats) {
+    if (!E || !v) return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_expv_solve: NULL argument");
+    cufsp_status s = CUFSP_SUCCESS;
+    while (E->t_now < E->t_final) {  // KryExpvFSP::solve, src/KryExpvFSP.cu:184-188
+        s = expv_step(E, v, (cudaStream_t)stream);
+        if (s != CUFSP_SUCCESS) break;
+    }
+    if (s == CUFSP_SUCCESS) {
+        cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+        if (e != cudaSuccess) s = cuda_error(e, "cufsp_expv_solve");
+    }
+    if (stats) *stats = E->stats;
+    return s;
+}
+
+extern "C" cufsp_status cufsp_expv_reset_time(cufsp_expv *E) {
+    if (!E) return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_expv_reset_time: NULL argument");
+    E->t_now = 0.0;  // the current vector is kept (src/KryExpvFSP.h:82-84)
+    return CUFSP_SUCCESS;
+}
+
+extern "C" cufsp_status cufsp_expv_final_time_reached(const cufsp_expv *E, int *reached) {
+    if (!E || !reached) return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_expv_final_time_reached: NULL argument");
+    *reached = E->t_now >= E->t_final;
+    return CUFSP_SUCCESS;
+}
+
+extern "C" cufsp_status cufsp_expv_get_stats(const cufsp_expv *E, cufsp_expv_stats *stats) {
+    if (!E || !stats) return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_expv_get_stats: NULL argument");
+    *stats = E->stats;
+    return CUFSP_SUCCESS;
+}

@@ -1,0 +1,171 @@
+/*
+ * cufsp.h -- C ABI of the B200-native Finite State Projection (FSP) engine.
+ *
+ * Every entry point returns a cufsp_status and never exits the process.  Device pointers are
+ * plain `double*` / `int*` in device memory; host pointers are stated as such.  Work is
+ * ordered on the `stream` argument (0 = the legacy default stream) and no call synchronises
+ * unless its comment says so.  Handles are not thread-safe: use one handle per host thread.
+ *
+ * Generator convention (shared by all formats):
+ *   (A p)(x) = sum_r c_r(t) [ a_r(x - nu_r) p(x - nu_r) 1{x - nu_r in box} - a_r(x) p(x) ]
+ * States are the hyper-rectangle 0 <= x_s <= b_s, indexed mixed-radix with species 0 fastest.
+ * The diagonal keeps the full outflow even where x + nu_r leaves the box, so 1 - sum(p) is the
+ * FSP truncation error.
+ */
+#ifndef CUFSP_H
+#define CUFSP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st *cufsp_stream_t; /* == cudaStream_t */
+
+typedef enum {
+    CUFSP_SUCCESS = 0,
+    CUFSP_ERR_INVALID_ARG = 1,  /* bad argument (null pointer, negative bound, ...) */
+    CUFSP_ERR_OVERFLOW = 2,     /* state count does not fit in int32 (the reference's index type) */
+    CUFSP_ERR_ALLOC = 3,        /* device or pinned allocation failed */
+    CUFSP_ERR_CUDA = 4,         /* a CUDA runtime call failed; see cufsp_last_error() */
+    CUFSP_ERR_NONFINITE = 5,    /* NaN/Inf met in coefficients, tables or the Krylov iteration */
+    CUFSP_ERR_STEP_LIMIT = 6,   /* Krylov max_nstep / max_reject exhausted */
+    CUFSP_ERR_UNSUPPORTED = 7,  /* valid request this build does not implement (e.g. > 32 reactions on KRONECKER) */
+    CUFSP_ERR_NO_DEVICE = 8     /* no CUDA device / kernels not loadable */
+} cufsp_status;
+
+/* Matrix formats, numbered as the reference's cuFSP::MatrixFormat (src/FSPMat.h:17-19).
+ * CSR and HYB are both served by the reaction-major propensity-table format (sparse variant);
+ * KRONECKER is the matrix-free factorised kernel. */
+typedef enum { CUFSP_FORMAT_CSR = 0, CUFSP_FORMAT_HYB = 1, CUFSP_FORMAT_KRONECKER = 2 } cufsp_format;
+
+/* Device propensity a_r(x): replaces cuFSP::PropFun (src/cme_util.h:25).  Must be a __device__
+ * function address taken (cudaMemcpyFromSymbol) in the SAME device-linked module as this
+ * library's kernels, i.e. a program linked against libcufsp_static.a with -rdc. */
+typedef double (*cufsp_prop_fn)(int *x, int reaction);
+/* Host propensity factor f_{r,s}(x_s): replaces cuFSP::PropFactorFun (src/fspmat_kron_kernels.h:13). */
+typedef double (*cufsp_prop_factor_fn)(int x, int species, int reaction);
+/* Host time coefficients c_r(t) -> out[n_reactions]: replaces cuFSP::TcoefFun (src/FSPMat.h:16),
+ * with a user pointer added so C callers can carry state. */
+typedef void (*cufsp_tcoef_fn)(double t, double *out, void *user);
+
+/* Model description (all pointers host memory; copied at create).
+ * Stoichiometry: CSR with one row per reaction and one column per species (the reference's
+ * CSRMatInt stoich argument, src/FSPMat.h:44-50).
+ * Propensity source, first non-null wins:
+ *   factor_tables : n_reactions * sum_s (b_s + 1) doubles, reaction-major then species then
+ *                   x_s = 0..b_s (the layout of SDKronMatSet::vals, src/fspmat_kron_kernels.cu:170-190)
+ *   prop_factor   : host factor function, evaluated into such tables at create
+ *   prop_device   : device propensity (sparse formats only)
+ * tcoef: c_r(t) callback used by cufsp_mat_action; NULL means c_r = 1. */
+typedef struct {
+    int n_species;
+    int n_reactions;
+    const int *fsp_bounds;
+    const int *stoich_vals;
+    const int *stoich_colidxs;
+    const int *stoich_rowptrs;
+    const double *factor_tables;
+    cufsp_prop_factor_fn prop_factor;
+    cufsp_prop_fn prop_device;
+    cufsp_tcoef_fn tcoef;
+    void *tcoef_user;
+} cufsp_model_desc;
+
+typedef struct cufsp_mat_s cufsp_mat;
+typedef struct cufsp_expv_s cufsp_expv;
+
+/* ---- status ---------------------------------------------------------------------------- */
+const char *cufsp_status_string(cufsp_status s);
+/* Detail of the last failure on this host thread ("" if none). */
+const char *cufsp_last_error(void);
+
+/* ---- state indexing (host) ----------------------------------------------------------------
+ * rect_fsp_num_states / indx2state / state2indx, src/cme_util.cu:5-22,55-62 */
+cufsp_status cufsp_num_states(int n_species, const int *fsp_bounds, int64_t *n_states);
+cufsp_status cufsp_indx2state(int64_t indx, int *state, int n_species, const int *fsp_bounds);
+cufsp_status cufsp_state2indx(const int *state, int n_species, const int *fsp_bounds, int64_t *indx);
+
+/* ---- state enumeration (device) -----------------------------------------------------------
+ * fsp_get_states, src/cme_util.cu:24-41: d_states[i*n_species + s] = x_s of state i (AoS int32).
+ * fsp_bounds is host memory. */
+cufsp_status cufsp_get_states(int n_species, const int *fsp_bounds, int *d_states, cufsp_stream_t stream);
+
+/* ---- generator ----------------------------------------------------------------------------
+ * cufsp_mat_create replaces both cuFSP::FSPMat constructors (src/FSPMat.cu:10-45 with PropFun,
+ * src/FSPMat.cu:49-76 with PropFactorFun).  Synchronises the device once (assembly). */
+cufsp_status cufsp_mat_create(const cufsp_model_desc *desc, cufsp_format format, cufsp_mat **out);
+cufsp_status cufsp_mat_destroy(cufsp_mat *A);
+/* get_n_rows / get_n_species / get_n_reactions, src/FSPMat.cu:108-118 */
+cufsp_status cufsp_mat_num_states(const cufsp_mat *A, int64_t *n_states);
+cufsp_status cufsp_mat_dims(const cufsp_mat *A, int *n_species, int *n_reactions, cufsp_format *format);
+
+/* FSPMat::action(t, x, y), src/FSPMat.cu:102-105: y += A(t) x with c_r = tcoef(t).
+ * x, y: device, n_states doubles, must not overlap. */
+cufsp_status cufsp_mat_action(cufsp_mat *A, double t, const double *x, double *y, cufsp_stream_t stream);
+
+/* General form: y = alpha * (sum_r coefs[r] A_r) x + beta * y, beta in {0, 1}.
+ * coefs: host, n_reactions doubles (NULL: use tcoef(t)).  Used by the Krylov and BDF drivers. */
+cufsp_status cufsp_mat_apply(cufsp_mat *A, double t, const double *coefs, double alpha, const double *x,
+                             double beta, double *y, cufsp_stream_t stream);
+
+/* FSPMat::action with HOST buffers: y_host += A(t) x_host.  Copies in, computes and copies out in
+ * a pipeline of slabs on internal streams; returns after y_host is written (synchronous).
+ * x_host / y_host should be pinned (cudaHostAlloc) for full PCIe bandwidth. */
+cufsp_status cufsp_mat_action_host(cufsp_mat *A, double t, const double *x_host, double *y_host);
+
+/* Sparse-format export for checking (HYB/CSR formats only): props[r*n + i] = a_r(x_i). */
+cufsp_status cufsp_mat_export_propensities(const cufsp_mat *A, double *d_props, cufsp_stream_t stream);
+
+/* ---- Krylov exp(tA)v -------------------------------------------------------------------------
+ * Replaces cuFSP::KryExpvFSP (src/KryExpvFSP.h:20-108, src/KryExpvFSP.cu:6-203).
+ * The Arnoldi basis, the Hessenberg matrix and all reductions stay on the device; one
+ * device->host read of the (m+2)^2 Hessenberg matrix per step drives the host step control. */
+typedef struct {
+    int64_t n_steps;     /* accepted steps */
+    int64_t n_reject;    /* rejected step attempts */
+    int64_t n_matvec;    /* generator applications */
+    int64_t n_breakdown; /* happy breakdowns */
+    double t_now;        /* time reached */
+    double last_err;     /* last local error estimate */
+} cufsp_expv_stats;
+
+/* Generic matvec for the MVFun constructor form (src/KryExpvFSP.h:15): y += A x into a
+ * zeroed y, device pointers, ordered on `stream`.  Return 0 on success. */
+typedef int (*cufsp_matvec_fn)(const double *x, double *y, void *user, cufsp_stream_t stream);
+
+/* n: vector length; m: Krylov dimension (1..60); tol; iop / q_iop: incomplete orthogonalisation
+ * against the last q_iop vectors; anorm: the ||A|| estimate of the reference (default 1.0). */
+cufsp_status cufsp_expv_create(int64_t n, int m, double tol, int iop, int q_iop, double anorm,
+                               cufsp_expv **out);
+cufsp_status cufsp_expv_destroy(cufsp_expv *E);
+/* max_nstep (reference default 10000) and max_reject (reference default 1000), KryExpvFSP.h:68-69 */
+cufsp_status cufsp_expv_set_limits(cufsp_expv *E, int64_t max_nstep, int64_t max_reject);
+/* Bind the operator: a generator (evaluated at time t_mat with its tcoef) or a callback. */
+cufsp_status cufsp_expv_bind_mat(cufsp_expv *E, cufsp_mat *A, double t_mat);
+cufsp_status cufsp_expv_bind_matvec(cufsp_expv *E, cufsp_matvec_fn fn, void *user);
+/* Bind the operator with explicit per-reaction coefficients (host, n_reactions doubles). */
+cufsp_status cufsp_expv_bind_mat_coefs(cufsp_expv *E, cufsp_mat *A, const double *coefs);
+/* KryExpvFSP::solve / step / reset_time / final_time_reached, KryExpvFSP.h:80-101.
+ * v: device vector (in: start vector, out: exp(t_final A) v).  Synchronous per step. */
+cufsp_status cufsp_expv_set_final_time(cufsp_expv *E, double t_final);
+cufsp_status cufsp_expv_solve(cufsp_expv *E, double *v, cufsp_stream_t stream, cufsp_expv_stats *stats);
+cufsp_status cufsp_expv_step(cufsp_expv *E, double *v, cufsp_stream_t stream);
+cufsp_status cufsp_expv_reset_time(cufsp_expv *E);
+cufsp_status cufsp_expv_final_time_reached(const cufsp_expv *E, int *reached);
+cufsp_status cufsp_expv_get_stats(const cufsp_expv *E, cufsp_expv_stats *stats);
+
+/* Dense exponential of a k x k column-major host matrix by scaling-and-squaring Pade(13,13)
+ * (replaces arma::expmat at src/KryExpvFSP.cu:125). */
+cufsp_status cufsp_expm_host(int k, const double *A, double *F);
+
+/* ---- vector helpers (device) ------------------------------------------------------------- */
+/* sum of x (deterministic order); result written to host *out; synchronises `stream`. */
+cufsp_status cufsp_vec_sum(int64_t n, const double *x, double *out, cufsp_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CUFSP_H */

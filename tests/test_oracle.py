@@ -1,0 +1,129 @@
+"""The FP64 host oracle, pinned against the reference's own code and its known-answer tests (CPU)."""
+import numpy as np
+import pytest
+
+import oracle
+from cuda_fsp_b200 import models
+
+
+def test_enumeration_known_answer():
+    """tests/test_fsp_get_states.cu:21-54: bounds (1023, 1023, 3), species 0 fastest, bit-exact."""
+    b = [1023, 1023, 3]
+    st = oracle.get_states(b)
+    assert st.shape == (1024 * 1024 * 4, 3)
+    x2, x1, x0 = np.meshgrid(np.arange(4), np.arange(1024), np.arange(1024), indexing="ij")
+    expect = np.stack([x0.ravel(), x1.ravel(), x2.ravel()], axis=1).astype(np.int32)
+    assert np.array_equal(st, expect)
+
+
+@pytest.mark.parametrize("bounds", [[3, 4, 2], [0, 5], [7], [1, 1, 1, 127, 127], [30, 2, 0, 4]])
+def test_indexing_matches_reference_host_code(bounds):
+    """indx2state / state2indx / rect_fsp_num_states (src/cme_util.cu:5-22,55-62) run from the
+    reference's own compiled objects, against the restatement."""
+    R = oracle.ref()
+    if R is None:
+        pytest.skip("reference shim not built (reference sources absent)")
+    b = np.asarray(bounds, np.int32)
+    n = oracle.num_states(b)
+    assert R.ref_num_states(len(b), b.ctypes.data) == n
+    st = oracle.get_states(b)
+    rng = np.random.default_rng(1)
+    idx = np.unique(np.concatenate([[0, n - 1], rng.integers(0, n, size=min(n, 500))]))
+    for i in idx:
+        s = np.empty(len(b), np.int32)
+        R.ref_indx2state(int(i), s.ctypes.data, len(b), b.ctypes.data)
+        assert np.array_equal(s, st[i])
+        assert R.ref_state2indx(s.ctypes.data, len(b), b.ctypes.data) == i
+        assert oracle.state2indx(s, b) == i
+
+
+def test_factor_table_layout_matches_reference():
+    """fspmat_sdkron_fill_host_data (src/fspmat_kron_kernels.cu:170-190) fills the same table
+    layout the product consumes, and its offsets are -nu."""
+    R = oracle.ref()
+    if R is None:
+        pytest.skip("reference shim not built (reference sources absent)")
+    for m in (models.toggle((31, 31)), models.gene_expression((1, 1, 1, 7, 9)), models.mass_action_3(6)):
+        b = np.asarray(m.bounds, np.int32)
+        sv, sc, sr = m.stoich_csr()
+        vals = np.empty_like(m.tables)
+        offs = np.empty((m.nr, m.ns), np.int32)
+        tab = np.ascontiguousarray(m.tables)
+        R.ref_sdkron_fill(m.ns, b.ctypes.data, m.nr, sv.ctypes.data, sc.ctypes.data, sr.ctypes.data,
+                          tab.ctypes.data, vals.ctypes.data, offs.ctypes.data)
+        assert np.array_equal(vals, m.tables)
+        assert np.array_equal(offs, -m.nu)
+
+
+def test_toggle_tables_from_oracle_match_model():
+    m = models.toggle((31, 31))
+    assert np.array_equal(oracle.toggle_factor_tables([31, 31]), m.tables)
+
+
+def test_csr_zero_vector_and_cross_format():
+    """tests/test_fsp_mat.cu:153-201: A*0 = 0; the propensity-function CSR and the factor-table
+    (Kronecker) form agree to 1e-14 in l2 at x = 1."""
+    m = models.toggle((31, 31))
+    c = m.coefs(1.0)
+    A_fun = oracle.assemble_model(m, oracle.PROP_TOGGLE)
+    A_tab = oracle.assemble_model(m, oracle.PROP_TABLES)
+    n = m.n_states
+    assert np.abs(A_fun.spmv(c, np.zeros(n))).sum() == 0.0
+    y1 = A_fun.spmv(c, np.ones(n))
+    y2 = A_tab.spmv(c, np.ones(n))
+    assert np.linalg.norm(y1 - y2) <= 1e-14
+
+
+def test_csr_structure():
+    """Per-reaction CSR rows hold the diagonal -a_r(x) and a_r(x - nu_r) in column order
+    (src/fspmat_csr_kernels.cu:53-94); column sums are <= 0 (probability leaks at the boundary)."""
+    m = models.birth_death_2()
+    A = oracle.assemble_model(m)
+    for r in range(m.nr):
+        rp = A.rowptr[r]
+        assert rp[0] == 0 and np.all(np.diff(rp) >= 1) and np.all(np.diff(rp) <= 2)
+        rows, cols, vals = A.entries(r)
+        assert np.all(np.diff(rows * (m.n_states + 1) + cols) > 0)  # sorted, unique per row
+        d = rows == cols
+        assert np.all(vals[d] <= 0) and np.all(vals[~d] >= 0)
+    S = A.to_scipy(m.coefs(0))
+    assert np.asarray(S.sum(axis=0)).max() <= 1e-12
+
+
+def test_oracle_expm_matches_scipy():
+    import scipy.linalg as sla
+    rng = np.random.default_rng(0)
+    for k, s in [(4, 0.1), (32, 3.0), (32, 50.0)]:
+        A = rng.standard_normal((k, k)) * s
+        E = sla.expm(A)
+        assert np.abs(oracle.expm(A) - E).max() <= 1e-12 * np.abs(E).max()
+
+
+def test_oracle_expv_matches_scipy_expm_multiply():
+    import scipy.sparse.linalg as spla
+    m = models.birth_death_2()
+    A = oracle.assemble_model(m)
+    c = m.coefs(0)
+    w, st, rc = oracle.expv(A, c, 10.0, m.p0(), m=30, tol=1e-8)
+    assert rc == 0 and st["t_now"] == 10.0
+    ws = spla.expm_multiply(A.to_scipy(c) * 10.0, m.p0())
+    assert np.abs(w - ws).sum() <= 1e-8
+
+
+def test_oracle_mass_conservation_reference_case():
+    """tests/test_kry_expv.cu:80-110: toggle on 257^2 states, t = 8 h, m = 30, tol 1e-8, IOP q = 2;
+    |1 - sum v| <= 1e-10."""
+    m = models.toggle((256, 256))
+    A = oracle.assemble_model(m)
+    w, st, rc = oracle.expv(A, m.coefs(0), 8 * 3600.0, m.p0(), m=30, tol=1e-8, iop=True, q_iop=2)
+    assert rc == 0
+    assert abs(1.0 - w.sum()) <= 1e-10
+
+
+def test_oracle_step_limit_and_zero_vector():
+    m = models.birth_death_2()
+    A = oracle.assemble_model(m)
+    _, _, rc = oracle.expv(A, m.coefs(0), 10.0, m.p0(), m=30, tol=1e-8, max_nstep=2)
+    assert oracle.ORC_ERR[rc] == "STEP_LIMIT"
+    w, st, rc = oracle.expv(A, m.coefs(0), 10.0, np.zeros(m.n_states))
+    assert rc == 0 and not w.any()
