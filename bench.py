@@ -68,56 +68,68 @@ def profile_traffic() -> float | None:
 
 
 class ClockSampler:
-    """nvidia-smi samples during the timed region."""
+    """SM clock and clock-event reasons sampled through NVML every ~1 ms during the timed region
+    (read-only queries; nothing is set)."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-         "clocks_event_reasons.sw_power_cap")
+    REASONS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown", 0x4: "sw_power_cap"}
 
     def __init__(self, index: int):
         self.index = index
-        self.proc = None
-        self.lines: list[str] = []
+        self.samples: list[float] = []
+        self.reasons: set[str] = set()
+        self.smax = None
+        self._stop = threading.Event()
+        self.nvml = None
 
     def start(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
-        except FileNotFoundError:
-            self.proc = None
+            import pynvml
+            pynvml.nvmlInit()
+            self.nvml = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            self.smax = float(pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM))
+        except Exception:
+            self.nvml = None
+            return
+        self.t = threading.Thread(target=self._run, daemon=True)
+        self.t.start()
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def _run(self):
+        pv = self.nvml
+        while not self._stop.is_set():
+            try:
+                self.samples.append(float(pv.nvmlDeviceGetClockInfo(self.h, pv.NVML_CLOCK_SM)))
+                r = pv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                for bit, name in self.REASONS.items():
+                    if r & bit:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(0.001)
 
     def stop(self) -> dict:
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
+        if self.nvml is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvml unavailable"], "samples": 0}
+        self._stop.set()
         self.t.join(timeout=2)
-        sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                smax = float(f[2])
-            except ValueError:
-                continue
-            for nm, v in zip(names, f[5:9]):
-                if v.lower() == "active":
-                    reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        return {"sm_mhz": statistics.median(self.samples) if self.samples else None, "sm_max_mhz": self.smax,
+                "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+def nvml_index(dev) -> int:
+    """NVML index of a CUDA device (NVML ignores CUDA_VISIBLE_DEVICES): match the PCI bus id."""
+    try:
+        import pynvml
+        import torch
+        p = torch.cuda.get_device_properties(dev)
+        pynvml.nvmlInit()
+        for i in range(pynvml.nvmlDeviceGetCount()):
+            pci = pynvml.nvmlDeviceGetPciInfo(pynvml.nvmlDeviceGetHandleByIndex(i))
+            if pci.bus == p.pci_bus_id and pci.device == p.pci_device_id and pci.domain == p.pci_domain_id:
+                return i
+    except Exception:
+        pass
+    return 0
 
 
 def dist_setup():
@@ -206,7 +218,7 @@ def run_ours(args):
     n = m.n_states
     A = FSPMat.from_model(m, MatrixFormat.KRONECKER)
     c = m.coefs(0)
-    n_sets = 4  # rotate 4 (x, y) pairs = 1.07 GB > 126 MB L2 between timed iterations
+    n_sets = args.sets  # default 4 rotating (x, y) pairs = 1.07 GB > 126 MB L2 between timed iterations
     g = torch.Generator(device=dev).manual_seed(1234 + rank)
     xs = [torch.rand(n, dtype=torch.float64, device=dev, generator=g) for _ in range(n_sets)]
     ys = [torch.zeros(n, dtype=torch.float64, device=dev) for _ in range(n_sets)]
@@ -217,12 +229,18 @@ def run_ours(args):
 
     for i in range(max(3, args.warmup)):
         step(i)
-    torch.cuda.synchronize(dev)
+    # keep warming up (untimed) for ~0.5 s so the SM clock has left its idle state
+    t_w = time.perf_counter()
+    i = 0
+    while not args.no_extras and time.perf_counter() - t_w < 0.5:
+        for _ in range(50):
+            step(i)
+            i += 1
+        torch.cuda.synchronize(dev)
     if world > 1:
         dist.barrier()
-    clocks = ClockSampler(torch.cuda.current_device())
+    clocks = ClockSampler(nvml_index(dev))
     clocks.start()
-    time.sleep(0.3)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize(dev)
     ev0.record(stream)
@@ -239,6 +257,13 @@ def run_ours(args):
     clk = clocks.stop()
     kernel_gbs = BYTES_PER_STATE * n / (ms * 1e-3) / 1e9
     value = kernel_gbs * world
+    if args.no_extras:  # profiling runs: the timed generator action only
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": round(value, 3), "unit": "GB/s", "ms_per_step": round(ms, 5),
+                              "steps": args.steps, "sets": n_sets, "profiling_run": True}), flush=True)
+        if world > 1:
+            dist.destroy_process_group()
+        return
 
     # e2e through the host-buffer entry point (pinned host memory, copies inside the timed region)
     xh = torch.empty(n, dtype=torch.float64).pin_memory()
@@ -292,9 +317,12 @@ def run_ours(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--sets", type=int, default=4, help="rotating (x, y) input pairs")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="time the generator action only (no e2e, expmv or CPU legs); for profiling runs")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -76,6 +76,7 @@ SIGNATURES = {
     "cufsp_mat_apply": [_P, C.c_double, _DP, C.c_double, _P, C.c_double, _P, _P],
     "cufsp_mat_action_host": [_P, C.c_double, _P, _P],
     "cufsp_mat_export_propensities": [_P, _P, _P],
+    "cufsp_mat_watchdog": [_P, _IP],
     "cufsp_expv_create": [C.c_int64, C.c_int, C.c_double, C.c_int, C.c_int, C.c_double, C.POINTER(_P)],
     "cufsp_expv_destroy": [_P],
     "cufsp_expv_set_limits": [_P, C.c_int64, C.c_int64],

@@ -102,6 +102,8 @@ void kron_destroy(KronData *k);
 cufsp_status kron_apply(KronData *k, const double *coefs, double alpha, const double *d_alpha,
                         const int *d_skip, const double *x, bool accumulate, double *y, cudaStream_t st,
                         int64_t i_begin = 0, int64_t i_end = -1);
+// Watchdog of the TMA-fed kernel: 1 if a bounded barrier wait expired since the last call (reset).
+int kron_watchdog(KronData *k);
 // halo (max |shift|) and slab granularity for the host-buffer pipeline
 int64_t kron_halo(const KronData *k);
 int64_t kron_row_len(const KronData *k);

@@ -5,69 +5,188 @@
 //                                - x[i]       * prod_s f_{r,s}(x_s) )
 // with d_r = sum_s nu_{r,s} * stride_s.
 //
-// Design (B200, FP64, HBM-bound):
+// Design (B200, FP64, HBM-bound; the only DRAM traffic is x once and y once or twice):
 //  * The state index is split as i = q * L + p.  p (the "inner" position) covers the first k
-//    species, q (the "row") the rest.  Each warp owns a fixed chunk of 32*V inner positions for
-//    the whole launch and sweeps rows q = q0, q0 + S, q0 + 2S, ...: the inner factor products
-//    prod_{s<k} f_{r,s} for its V positions per lane are computed ONCE into registers.
-//  * Per row, lane r computes the row-uniform outer products prod_{s>=k} f_{r,s} (times c_r)
-//    for reaction r and publishes them through a per-warp shared-memory slot, so the per-state
-//    work is 3 FP64 ops + 1 gather per reaction; no integer division per state.
-//  * All warps of the grid sweep the rows in one global order (row stride S = warps / chunks),
-//    so the x planes addressed by the shifted gathers x[i - d_r] were brought into L2 by a
-//    neighbouring warp moments earlier: DRAM traffic stays at x once + y once (or twice when
-//    accumulating).  x is read through the read-only path, y with evict-first hints.
-//  * Gather addresses are clamped into [0, n); a neighbour outside the box has a zero
-//    coefficient (factor 0 from the inner or outer validity test), so no predicated loads sit
-//    between the address arithmetic and the FMAs and every load of a row is issued up front.
+//    species, q (the "row") the rest.  Each warp owns a fixed chunk of 32*V consecutive inner
+//    positions for the whole launch and sweeps rows q = q0, q0 + S, ...; the inner factor products
+//    prod_{s<k} f_{r,s} of its V positions per lane are computed once, into registers.
+//  * The row-uniform outer products G_r(q) = prod_{s>=k} f_{r,s} (and the shifted ones, zero when
+//    the outer part of x - nu_r leaves the box) are tabulated at create time (Q x NR doubles2, L2
+//    resident).  Per row, lane r reads G_r(q) once, multiplies by c_r, and publishes it through a
+//    per-warp shared-memory slot: no integer division or table walk per state or per row.
+//  * Per state and reaction the work is one gather x[i - d_r] and three FP64 operations; reaction
+//    counts are template parameters so no padded reaction costs anything.
+//  * All warps sweep the rows in one global order (row stride S = warps / chunks), so the planes
+//    addressed by the shifted gathers were brought into L2 by a neighbouring warp moments earlier.
+//    x is read through the read-only path, y with evict-first hints.
+//  * Gather indices are clamped into [0, n); a neighbour outside the box has a zero coefficient
+//    (zero inner factor or zero outer table entry), so all loads of a row issue up front.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
+#include <cstring>
 
 #include "cufsp_internal.h"
+#include "cufsp_march.h"
 
 namespace cufsp {
+
+constexpr int kKronThreads = 128;
+constexpr int kKronWarps = kKronThreads / 32;
 
 struct KronArgs {
     const double *__restrict__ tables;  // [nr][tab_stride]
     const int *__restrict__ nu;         // [nr][ns]
+    const double2 *__restrict__ gtab;   // [Q][NR] (shifted, unshifted) outer factor products
     const double *__restrict__ d_alpha; // nullable device scalar multiplying alpha
     const int *__restrict__ d_skip;     // nullable: return at once when *d_skip != 0
-    int64_t n;
+    int n;
     int tab_stride;
     int ns, nr, k;
     int L, n_chunks;
     int q_begin, q_end;
+    int q_safe_lo, q_safe_hi;  // rows whose gathers i - d_r all lie inside [0, n): no clamping
+    int pf_dist;               // L2 prefetch distance in row iterations (0: off)
     int dims[CUFSP_MAX_SPECIES];
     int tab_off[CUFSP_MAX_SPECIES];
     int delta[CUFSP_MAX_REACTIONS];
     double coef[CUFSP_MAX_REACTIONS];
+    int gid[CUFSP_MAX_REACTIONS];  // diagonal group of each reaction (same inner factor table)
+    int rep[CUFSP_MAX_REACTIONS];  // first reaction of each group
 };
 
-template <int NR, int V, bool ACCUM>
-__global__ void __launch_bounds__(256) k_kron_mv(const KronArgs a, const double *__restrict__ x,
-                                                 double *__restrict__ y) {
-    __shared__ double2 wsm[8][NR];
+// Asynchronous bulk prefetch of [p, p + bytes) into L2 by the TMA unit (16-byte granules).
+__device__ __forceinline__ void prefetch_l2_bulk(const void *p, unsigned bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// Prefetch this warp's chunk of row q of `v` (n doubles) into L2.  The bulk prefetch needs a
+// 16-byte aligned address and size, and v itself may be only 8-byte aligned (a Krylov basis
+// vector at an odd offset), so the byte range is shrunk to 16-byte boundaries inside [v, v + n).
+template <int V>
+__device__ __forceinline__ void prefetch_row_chunk(const double *v, int n, int q, int L, int p_chunk) {
+    const long long b = (long long)q * L + p_chunk;
+    long long e = b + 32 * V;
+    const long long row_end = (long long)(q + 1) * L;
+    if (e > row_end) e = row_end;
+    const unsigned long long base = reinterpret_cast<unsigned long long>(v);
+    const unsigned long long lo_lim = (base + 15ull) & ~15ull, hi_lim = (base + 8ull * (unsigned long long)n) & ~15ull;
+    unsigned long long lo = (base + 8ull * (unsigned long long)b) & ~15ull;
+    unsigned long long hi = (base + 8ull * (unsigned long long)e + 15ull) & ~15ull;
+    if (lo < lo_lim) lo = lo_lim;
+    if (hi > hi_lim) hi = hi_lim;
+    if (hi > lo) prefetch_l2_bulk(reinterpret_cast<const void *>(lo), (unsigned)(hi - lo));
+}
+
+// Loads of one row for one lane: x and y at i0 .. i0 + V - 1 and the gathers x[i0 + v - d_r]
+// (clamped into [0, n) unless SAFE, i.e. unless the row is known to keep them in range).
+template <int NR, int V, bool ACCUM, bool SAFE>
+__device__ __forceinline__ void kron_load_row(const KronArgs &a, const double *__restrict__ x,
+                                              const double *__restrict__ y, int i0, int nm1, double (&xv)[V],
+                                              double (&yv)[V], double (&xg)[NR][V]) {
+    if (V >= 2) {
+#pragma unroll
+        for (int v = 0; v < V; v += 2) {
+            const double2 t = __ldg(reinterpret_cast<const double2 *>(x + i0 + v));
+            xv[v] = t.x;
+            xv[(v + 1) % V] = t.y;
+            if (ACCUM) {
+                const double2 u = __ldcs(reinterpret_cast<const double2 *>(y + i0 + v));
+                yv[v] = u.x;
+                yv[(v + 1) % V] = u.y;
+            }
+        }
+    } else {
+        xv[0] = __ldg(x + i0);
+        if (ACCUM) yv[0] = __ldcs(y + i0);
+    }
+    const double *xb = x + i0;
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+        const int d = a.delta[r];
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            if (SAFE) {
+                xg[r][v] = __ldg(xb + (v - d));
+            } else {
+                const int src = min(max(i0 + v - d, 0), nm1);
+                xg[r][v] = __ldg(x + src);
+            }
+        }
+    }
+}
+
+// y[i0 + v] (+)= sum_r wa_r Fa_r x[i - d_r] - x[i] sum_g wb_g Fb_g for one row, where the
+// diagonal runs over groups g of reactions sharing one inner factor table.
+template <int NR, int NG, int V, bool ACCUM>
+__device__ __forceinline__ void kron_row_out(const double *wa, const double *wb, const double (&Fa)[V][NR],
+                                             const double (&Fb)[V][NG], const double (&xv)[V],
+                                             const double (&yv)[V], const double (&xg)[NR][V], double *yo) {
+    double acc[V], dg[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) acc[v] = dg[v] = 0.0;
+#pragma unroll
+    for (int g = 0; g < NG; ++g) {
+        const double w = wb[g];
+#pragma unroll
+        for (int v = 0; v < V; ++v) dg[v] = fma(w, Fb[v][g], dg[v]);
+    }
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+        const double w = wa[r];
+#pragma unroll
+        for (int v = 0; v < V; ++v) acc[v] = fma(w * Fa[v][r], xg[r][v], acc[v]);
+    }
+    double out[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v) {
+        out[v] = fma(-dg[v], xv[v], acc[v]);
+        if (ACCUM) out[v] += yv[v];
+    }
+    if (V >= 2) {
+#pragma unroll
+        for (int v = 0; v < V; v += 2)
+            __stcs(reinterpret_cast<double2 *>(yo + v), make_double2(out[v], out[(v + 1) % V]));
+    } else {
+        __stcs(yo, out[0]);
+    }
+}
+
+#ifndef CUFSP_KRON_MINB
+#define CUFSP_KRON_MINB 1
+#endif
+// Per-warp shared words per row: wa[NR] (shifted), wt[NR] (unshifted, per reaction), wb[NG] (grouped).
+template <int NR, int NG>
+struct KronRowWords {
+    static constexpr int kStride = 2 * NR + NG;
+};
+
+template <int NR, int NG, int V, bool ACCUM>
+__global__ void __launch_bounds__(kKronThreads, CUFSP_KRON_MINB) k_kron_mv(const KronArgs a, const double *__restrict__ x,
+                                                                          double *__restrict__ y) {
+    constexpr int RS = KronRowWords<NR, NG>::kStride;
+    __shared__ double wsm[kKronWarps][2 * RS];
     if (a.d_skip && *a.d_skip) return;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const int gwarp = blockIdx.x * 8 + wib;
-    const int nwarps = gridDim.x * 8;
+    const int gwarp = blockIdx.x * kKronWarps + wib;
+    const int nwarps = gridDim.x * kKronWarps;
     const int rstride = nwarps / a.n_chunks;
     const int chunk = gwarp % a.n_chunks;
     const int rowoff = gwarp / a.n_chunks;
     if (rowoff >= rstride) return;  // whole warp leaves; no CTA-wide barrier follows
 
     const int p0 = chunk * (32 * V) + lane * V;
-    const bool active = p0 < a.L;  // V == 2 only when L is even, so p0 + 1 < L as well
+    const bool active = p0 < a.L;  // L is a multiple of V, so p0 + V - 1 < L as well
 
-    // Inner factor products for this lane's V positions (fixed for the whole launch).
-    double Fa[V][NR], Fb[V][NR];
+    // Inner factor products of this lane's V positions, fixed for the whole launch: shifted ones per
+    // reaction (Fa) and unshifted ones per diagonal group (Fb, from the group's first reaction).
+    double Fa[V][NR], Fb[V][NG];
 #pragma unroll
     for (int v = 0; v < V; ++v) {
 #pragma unroll
-        for (int r = 0; r < NR; ++r) {
-            Fa[v][r] = (r < a.nr) ? 1.0 : 0.0;
-            Fb[v][r] = (r < a.nr) ? 1.0 : 0.0;
-        }
+        for (int r = 0; r < NR; ++r) Fa[v][r] = 1.0;
+#pragma unroll
+        for (int g = 0; g < NG; ++g) Fb[v][g] = 1.0;
         int rem = min(p0 + v, a.L - 1);
         for (int s = 0; s < a.k; ++s) {
             const int d = a.dims[s];
@@ -76,94 +195,93 @@ __global__ void __launch_bounds__(256) k_kron_mv(const KronArgs a, const double 
             const double *t = a.tables + a.tab_off[s];
 #pragma unroll
             for (int r = 0; r < NR; ++r) {
-                if (r < a.nr) {
-                    const double *tr = t + (size_t)r * a.tab_stride;
-                    Fb[v][r] *= __ldg(tr + xs);
-                    const int xsh = xs - __ldg(a.nu + r * a.ns + s);
-                    Fa[v][r] = (xsh < 0 || xsh >= d) ? 0.0 : Fa[v][r] * __ldg(tr + xsh);
-                }
+                const double *tr = t + r * a.tab_stride;
+                const int xsh = xs - __ldg(a.nu + r * a.ns + s);
+                Fa[v][r] = (xsh < 0 || xsh >= d) ? 0.0 : Fa[v][r] * __ldg(tr + xsh);
             }
+#pragma unroll
+            for (int g = 0; g < NG; ++g) Fb[v][g] *= __ldg(t + a.rep[g] * a.tab_stride + xs);
         }
     }
 
-    const double alpha_dev = a.d_alpha ? __ldg(a.d_alpha) : 1.0;
-    const int64_t nm1 = a.n - 1;
-    double2 *myw = wsm[wib];
-    for (int q = a.q_begin + rowoff; q < a.q_end; q += rstride) {
-        // Row-uniform outer factors, one reaction per lane.
-        if (lane < NR) {
-            double wa = 0.0, wb = 0.0;
-            if (lane < a.nr) {
-                double ga = 1.0, gb = 1.0;
-                bool ok = true;
-                int rem = q;
-                const double *tr = a.tables + (size_t)lane * a.tab_stride;
-                for (int s = a.k; s < a.ns; ++s) {
-                    const int d = a.dims[s];
-                    const int xs = rem % d;
-                    rem /= d;
-                    const double *t = tr + a.tab_off[s];
-                    gb *= __ldg(t + xs);
-                    const int xsh = xs - __ldg(a.nu + lane * a.ns + s);
-                    if (xsh < 0 || xsh >= d) ok = false;
-                    else ga *= __ldg(t + xsh);
-                }
-                const double c = a.coef[lane] * alpha_dev;
-                wa = ok ? c * ga : 0.0;
-                wb = c * gb;
-            }
-            myw[lane] = make_double2(wa, wb);
+    const double cl = (lane < NR) ? a.coef[lane] * (a.d_alpha ? __ldg(a.d_alpha) : 1.0) : 0.0;
+    const int my_gid = (lane < NR) ? a.gid[lane] : -1;
+    const int nm1 = a.n - 1;
+    double *myw = wsm[wib];
+    // The grid sweeps the rows in one global order with stride rstride.
+    int q = a.q_begin + rowoff;
+    const int q_stop = a.q_end, qstep = rstride;
+    const int p_chunk = chunk * (32 * V);
+    if (lane == 0) {  // start the L2 prefetch pipeline: the first pf_dist rows of this warp
+        for (int d = 0; d < a.pf_dist; ++d) {
+            const int qq = q + d * qstep;
+            if (qq >= q_stop) break;
+            prefetch_row_chunk<V>(x, a.n, qq, a.L, p_chunk);
+            if (ACCUM) prefetch_row_chunk<V>(y, a.n, qq, a.L, p_chunk);
         }
+    }
+    // Two rows per iteration (q and q + qstep): twice the independent loads in flight per warp.
+    double2 gA = make_double2(0.0, 0.0), gB = gA;
+    if (lane < NR && q < q_stop) gA = __ldg(a.gtab + (size_t)q * NR + lane);
+    if (lane < NR && q + qstep < q_stop) gB = __ldg(a.gtab + (size_t)(q + qstep) * NR + lane);
+    for (; q < q_stop; q += 2 * qstep) {
+        const int q2 = q + qstep;
+        const bool has2 = q2 < q_stop;
+        const double2 g0 = gA, g1 = gB;
+        if (lane < NR && q + 2 * qstep < q_stop) gA = __ldg(a.gtab + (size_t)(q + 2 * qstep) * NR + lane);
+        if (lane < NR && q + 3 * qstep < q_stop) gB = __ldg(a.gtab + (size_t)(q + 3 * qstep) * NR + lane);
+        if (lane == 0 && a.pf_dist > 0) {
+            for (int d = 0; d < 2; ++d) {
+                const int qq = q + (a.pf_dist + d) * qstep;
+                if (qq < q_stop) {
+                    prefetch_row_chunk<V>(x, a.n, qq, a.L, p_chunk);
+                    if (ACCUM) prefetch_row_chunk<V>(y, a.n, qq, a.L, p_chunk);
+                }
+            }
+        }
+        const int i0 = q * a.L + p0, i1 = q2 * a.L + p0;
+        // warp-uniform: both rows' gathers stay inside [0, n) -> no clamping code
+        const bool safe = q >= a.q_safe_lo && (has2 ? q2 : q) < a.q_safe_hi;
+        double xv0[V], yv0[V], xg0[NR][V], xv1[V], yv1[V], xg1[NR][V];
+        if (active) {
+            if (safe) {
+                kron_load_row<NR, V, ACCUM, true>(a, x, y, i0, nm1, xv0, yv0, xg0);
+                if (has2) kron_load_row<NR, V, ACCUM, true>(a, x, y, i1, nm1, xv1, yv1, xg1);
+            } else {
+                kron_load_row<NR, V, ACCUM, false>(a, x, y, i0, nm1, xv0, yv0, xg0);
+                if (has2) kron_load_row<NR, V, ACCUM, false>(a, x, y, i1, nm1, xv1, yv1, xg1);
+            }
+        }
+        // row words: wa_r = c_r Ga_r(q); wb_g = sum over the group's reactions of c_r Gb_r(q)
+        if (lane < NR) {
+            myw[lane] = cl * g0.x;
+            myw[RS + lane] = cl * g1.x;
+            if (NG == NR) {
+                myw[2 * NR + lane] = cl * g0.y;
+                myw[RS + 2 * NR + lane] = cl * g1.y;
+            } else {
+                myw[NR + lane] = cl * g0.y;
+                myw[RS + NR + lane] = cl * g1.y;
+            }
+        }
+        if (NG != NR) {
+            __syncwarp();
+            if (lane < NG) {
+                double s0 = 0.0, s1 = 0.0;
+                for (int r = 0; r < NR; ++r) {
+                    const bool mine = a.gid[r] == lane;
+                    s0 += mine ? myw[NR + r] : 0.0;
+                    s1 += mine ? myw[RS + NR + r] : 0.0;
+                }
+                myw[2 * NR + lane] = s0;
+                myw[RS + 2 * NR + lane] = s1;
+            }
+        }
+        (void)my_gid;
         __syncwarp();
         if (active) {
-            const int64_t i0 = (int64_t)q * a.L + p0;
-            double xv[V], yv[V];
-            if (V == 2) {
-                const double2 t = __ldg(reinterpret_cast<const double2 *>(x + i0));
-                xv[0] = t.x;
-                xv[V - 1] = t.y;
-                if (ACCUM) {
-                    const double2 u = __ldcs(reinterpret_cast<const double2 *>(y + i0));
-                    yv[0] = u.x;
-                    yv[V - 1] = u.y;
-                }
-            } else {
-                xv[0] = __ldg(x + i0);
-                if (ACCUM) yv[0] = __ldcs(y + i0);
-            }
-            double xg[NR][V];
-#pragma unroll
-            for (int r = 0; r < NR; ++r) {
-#pragma unroll
-                for (int v = 0; v < V; ++v) {
-                    int64_t src = i0 + v - a.delta[r];
-                    src = src < 0 ? 0 : (src > nm1 ? nm1 : src);
-                    xg[r][v] = __ldg(x + src);
-                }
-            }
-            double acc[V], dg[V];
-#pragma unroll
-            for (int v = 0; v < V; ++v) acc[v] = dg[v] = 0.0;
-#pragma unroll
-            for (int r = 0; r < NR; ++r) {
-                const double2 w = myw[r];
-#pragma unroll
-                for (int v = 0; v < V; ++v) {
-                    dg[v] = fma(w.y, Fb[v][r], dg[v]);
-                    acc[v] = fma(w.x * Fa[v][r], xg[r][v], acc[v]);
-                }
-            }
-            double out[V];
-#pragma unroll
-            for (int v = 0; v < V; ++v) {
-                out[v] = fma(-dg[v], xv[v], acc[v]);
-                if (ACCUM) out[v] += yv[v];
-            }
-            if (V == 2) {
-                __stcs(reinterpret_cast<double2 *>(y + i0), make_double2(out[0], out[V - 1]));
-            } else {
-                __stcs(y + i0, out[0]);
-            }
+            kron_row_out<NR, NG, V, ACCUM>(myw, myw + 2 * NR, Fa, Fb, xv0, yv0, xg0, y + i0);
+            if (has2) kron_row_out<NR, NG, V, ACCUM>(myw + RS, myw + RS + 2 * NR, Fa, Fb, xv1, yv1, xg1, y + i1);
         }
         __syncwarp();
     }
@@ -171,46 +289,217 @@ __global__ void __launch_bounds__(256) k_kron_mv(const KronArgs a, const double 
 
 struct KronData {
     int64_t n = 0;
-    int ns = 0, nr = 0, k = 0, L = 0, Q = 0, V = 1, NR = 4, n_chunks = 1;
+    int ns = 0, nr = 0, k = 0, L = 0, Q = 0, V = 1, NR = 1, n_chunks = 1;
     int tab_stride = 0;
     double *d_tables = nullptr;
     int *d_nu = nullptr;
+    double2 *d_gtab = nullptr;
     std::vector<int> dims, tab_off, delta;
     int64_t halo = 0;
     int grid_full = 0;
+    int q_safe_lo = 0, q_safe_hi = 0;
+    int pf_dist = 4;
+    int NG = 1;                         // diagonal groups as compiled (2, 4 or NR)
+    std::vector<int> gid, rep;          // per reaction / per group
+    // TMA-fed marching fast path (cufsp_kron_march.cu)
+    bool march = false;
+    MarchArgs ma;       // constant part of the launch arguments
+    int march_V = 1, march_threads = 0, march_grid = 0;
+    size_t march_smem = 0;
+    int *d_err = nullptr;
+    double2 *d_gtab_march = nullptr;  // only when the marching split differs from k
 };
+
+// Outer factor table for the inner split k: G[q][r] = (prod_{s>=k} f_{r,s}(x_s - nu_{r,s}), or 0
+// when that leaves the box; prod_{s>=k} f_{r,s}(x_s)) for every row q of n / prod_{s<k} n_s.
+static std::vector<double2> outer_table(const ModelHost &m, const KronData *kd, int k) {
+    int64_t L = 1;
+    for (int s = 0; s < k; ++s) L *= kd->dims[s];
+    const int64_t Q = m.n / L;
+    std::vector<double2> g((size_t)Q * kd->NR, make_double2(0.0, 0.0));
+    std::vector<int> xs(m.ns, 0);
+    for (int64_t q = 0; q < Q; ++q) {
+        int64_t rem = q;
+        for (int s = k; s < m.ns; ++s) {
+            xs[s] = (int)(rem % kd->dims[s]);
+            rem /= kd->dims[s];
+        }
+        for (int r = 0; r < m.nr; ++r) {
+            const double *tr = m.tables.data() + (size_t)r * m.tab_stride;
+            double ga = 1.0, gb = 1.0;
+            bool ok = true;
+            for (int s = k; s < m.ns; ++s) {
+                const double *t = tr + m.tab_off[s];
+                gb *= t[xs[s]];
+                const int xsh = xs[s] - m.nu[(size_t)r * m.ns + s];
+                if (xsh < 0 || xsh >= kd->dims[s]) ok = false;
+                else ga *= t[xsh];
+            }
+            g[(size_t)q * kd->NR + r] = make_double2(ok ? ga : 0.0, gb);
+        }
+    }
+    return g;
+}
+
+// Plan the marching kernel: the slowest species is the marching axis, rows of L = prod_{s<k} n_s
+// inner positions fill W = L / (32 V) warps exactly, plane shifts span at most 2 planes each way.
+static void plan_march(const ModelHost &m, KronData *kd) {
+    kd->march = false;
+    // Opt-in (CUFSP_KRON_MARCH=1): on the 255^3 mass-action workload this kernel still trails the
+    // register/L1 kernel (about 200 us vs 147 us), so the latter stays the default.
+    const char *ev = getenv("CUFSP_KRON_MARCH");
+    if (!ev || atoi(ev) == 0) return;
+    const int ns = m.ns;
+    if (ns < 2 || kd->NR > 16) return;
+    const int zs = ns - 1, Z = kd->dims[zs];
+    const int64_t P = m.n / Z;
+    int k = -1, V = 0, W = 0;
+    int64_t L = 1;
+    for (int kk = 1; kk <= zs && k < 0; ++kk) {
+        L *= kd->dims[kk - 1];
+        for (int vv = 1; vv <= 2 && k < 0; ++vv) {
+            if (vv == 2 && kd->NR > 12) continue;
+            if (L % (32 * vv) == 0 && L / (32 * vv) <= 8) {
+                k = kk;
+                V = vv;
+                W = (int)(L / (32 * vv));
+            }
+        }
+    }
+    if (k < 0 || P % L != 0 || (P % 2) != 0) return;
+    const int RP = (int)(P / L);
+    std::vector<int> dz(m.nr), drow(m.nr), dp(m.nr);
+    int hz_lo = 0, hz_hi = 0, hr_lo = 0, hr_hi = 0, gmax = 0;
+    for (int r = 0; r < m.nr; ++r) {
+        int64_t p = 0, row = 0, st = 1, rst = 1;
+        for (int s = 0; s < k; ++s) {
+            p += (int64_t)m.nu[(size_t)r * ns + s] * st;
+            st *= kd->dims[s];
+        }
+        for (int s = k; s < zs; ++s) {
+            row += (int64_t)m.nu[(size_t)r * ns + s] * rst;
+            rst *= kd->dims[s];
+        }
+        const int d = m.nu[(size_t)r * ns + zs];
+        if (std::llabs(p) >= L || std::llabs(row) >= RP || std::abs(d) > 2) return;  // not a near neighbour
+        dz[r] = d;
+        drow[r] = (int)row;
+        dp[r] = (int)p;
+        hz_lo = std::max(hz_lo, d);
+        hz_hi = std::max(hz_hi, -d);
+        hr_lo = std::max(hr_lo, (int)row);
+        hr_hi = std::max(hr_hi, (int)-row);
+        gmax = std::max(gmax, (int)std::llabs(p));
+    }
+    const int slots = hz_lo + hz_hi + 2;
+    if (slots > kMarchMaxSlots) return;
+    const int guard = std::max(2, (gmax + 1) & ~1);
+    const size_t budget = 100 * 1024;
+    int R = 0;
+    for (int cand : {8, 6, 4, 2, 1}) {  // <= kMarchMaxR; one outer-factor entry per thread
+        if (cand > RP || cand > kMarchMaxR || cand * kd->NR > 32 * W) continue;
+        const size_t se = 2 * (size_t)guard + (size_t)(cand + hr_lo + hr_hi) * L;
+        const size_t bytes = slots * se * 8 + (size_t)cand * kd->NR * 16;
+        if (bytes <= budget) {
+            R = cand;
+            break;
+        }
+    }
+    if (R == 0) return;
+    MarchArgs &a = kd->ma;
+    std::memset(&a, 0, sizeof(a));
+    a.n = (int)m.n;
+    a.P = (int)P;
+    a.L = (int)L;
+    a.RP = RP;
+    a.Z = Z;
+    a.ns = ns;
+    a.k = k;
+    a.tab_stride = m.tab_stride;
+    a.R = R;
+    a.hr_lo = hr_lo;
+    a.hr_hi = hr_hi;
+    a.hz_lo = hz_lo;
+    a.hz_hi = hz_hi;
+    a.slots = slots;
+    a.guard = guard;
+    a.slot_elems = 2 * guard + (R + hr_lo + hr_hi) * (int)L;
+    a.row_tiles = (RP + R - 1) / R;
+    for (int s = 0; s < CUFSP_MAX_SPECIES; ++s) {
+        a.dims[s] = s < ns ? kd->dims[s] : 1;
+        a.tab_off[s] = s < ns ? m.tab_off[s] : 0;
+    }
+    for (int r = 0; r < m.nr; ++r) {
+        a.dz[r] = dz[r];
+        a.soff[r] = (hr_lo - drow[r]) * (int)L - dp[r];
+    }
+    kd->march_V = V;
+    kd->march_threads = 32 * W;
+    kd->march_smem = (size_t)slots * a.slot_elems * 8 + (size_t)R * kd->NR * 16;
+    MarchKernel kern[2] = {pick_march_kernel(kd->NR, V, false), pick_march_kernel(kd->NR, V, true)};
+    if (!kern[0] || !kern[1]) return;
+    int occ = 0;
+    for (MarchKernel kf : kern) {
+        if (cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kd->march_smem) != cudaSuccess)
+            return;
+    }
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern[1], kd->march_threads, kd->march_smem) != cudaSuccess ||
+        occ < 1)
+        return;
+    const int resident = device_info().sm_count * occ;
+    const int zsegs = std::max(1, std::min(Z, resident / a.row_tiles));
+    a.zseg = (Z + zsegs - 1) / zsegs;
+    kd->march_grid = a.row_tiles * ((Z + a.zseg - 1) / a.zseg);
+    if (cudaMalloc(&kd->d_err, sizeof(int)) != cudaSuccess) return;
+    if (cudaMemset(kd->d_err, 0, sizeof(int)) != cudaSuccess) return;
+    kd->march = true;
+}
 
 using KronKernel = void (*)(const KronArgs, const double *, double *);
 
 template <int NR, int V>
-static KronKernel pick_accum(bool accum) {
-    return accum ? k_kron_mv<NR, V, true> : k_kron_mv<NR, V, false>;
+static KronKernel pick_ng(int NG, bool accum) {
+    if (NG == 2 && NR > 2) return accum ? k_kron_mv<NR, (NR > 2 ? 2 : NR), V, true> : k_kron_mv<NR, (NR > 2 ? 2 : NR), V, false>;
+    if (NG == 4 && NR > 4) return accum ? k_kron_mv<NR, (NR > 4 ? 4 : NR), V, true> : k_kron_mv<NR, (NR > 4 ? 4 : NR), V, false>;
+    return accum ? k_kron_mv<NR, NR, V, true> : k_kron_mv<NR, NR, V, false>;
 }
 
-static KronKernel pick_kernel(int NR, int V, bool accum) {
+#define KRON_CASE(NRv, Vv) \
+    case NRv:              \
+        return pick_ng<NRv, Vv>(NG, accum);
+
+// NG: diagonal groups as compiled (2, 4 or NR).
+static KronKernel pick_kernel(int NR, int NG, int V, bool accum) {
+    if (V == 4) {
+        switch (NR) {
+            KRON_CASE(1, 4) KRON_CASE(2, 4) KRON_CASE(3, 4) KRON_CASE(4, 4) KRON_CASE(5, 4) KRON_CASE(6, 4)
+            default: return nullptr;
+        }
+    }
     if (V == 2) {
         switch (NR) {
-            case 4: return pick_accum<4, 2>(accum);
-            case 8: return pick_accum<8, 2>(accum);
-            case 12: return pick_accum<12, 2>(accum);
-            case 16: return pick_accum<16, 2>(accum);
+            KRON_CASE(1, 2) KRON_CASE(2, 2) KRON_CASE(3, 2) KRON_CASE(4, 2) KRON_CASE(5, 2) KRON_CASE(6, 2)
+            KRON_CASE(7, 2) KRON_CASE(8, 2) KRON_CASE(9, 2) KRON_CASE(10, 2) KRON_CASE(11, 2) KRON_CASE(12, 2)
             default: return nullptr;
         }
     }
     switch (NR) {
-        case 4: return pick_accum<4, 1>(accum);
-        case 8: return pick_accum<8, 1>(accum);
-        case 12: return pick_accum<12, 1>(accum);
-        case 16: return pick_accum<16, 1>(accum);
-        case 24: return pick_accum<24, 1>(accum);
-        case 32: return pick_accum<32, 1>(accum);
+        KRON_CASE(1, 1) KRON_CASE(2, 1) KRON_CASE(3, 1) KRON_CASE(4, 1) KRON_CASE(5, 1) KRON_CASE(6, 1)
+        KRON_CASE(7, 1) KRON_CASE(8, 1) KRON_CASE(9, 1) KRON_CASE(10, 1) KRON_CASE(11, 1) KRON_CASE(12, 1)
+        KRON_CASE(13, 1) KRON_CASE(14, 1) KRON_CASE(15, 1) KRON_CASE(16, 1) KRON_CASE(20, 1) KRON_CASE(24, 1)
+        KRON_CASE(28, 1) KRON_CASE(32, 1)
         default: return nullptr;
     }
 }
+#undef KRON_CASE
+
+static int max_v_for(int NR) { return NR <= 6 ? 4 : (NR <= 12 ? 2 : 1); }
 
 cufsp_status kron_create(const ModelHost &m, KronData **out) {
     if (m.nr > CUFSP_MAX_REACTIONS)
         return set_error(CUFSP_ERR_UNSUPPORTED, "KRONECKER format supports at most 32 reactions");
+    if (m.n > (int64_t(1) << 30))  // gather indices i - d_r stay inside int32 for n <= 2^30
+        return set_error(CUFSP_ERR_UNSUPPORTED, "KRONECKER format supports at most 2^30 states");
     KronData *kd = new KronData();
     kd->n = m.n;
     kd->ns = m.ns;
@@ -219,7 +508,7 @@ cufsp_status kron_create(const ModelHost &m, KronData **out) {
     kd->tab_off = m.tab_off;
     kd->dims.resize(m.ns);
     for (int s = 0; s < m.ns; ++s) kd->dims[s] = m.bounds[s] + 1;
-    kd->NR = m.nr <= 4 ? 4 : m.nr <= 8 ? 8 : m.nr <= 12 ? 12 : m.nr <= 16 ? 16 : m.nr <= 24 ? 24 : 32;
+    kd->NR = m.nr <= 16 ? m.nr : (m.nr <= 20 ? 20 : m.nr <= 24 ? 24 : m.nr <= 28 ? 28 : 32);
 
     // Shifts d_r = sum_s nu_{r,s} * stride_s and the halo max |d_r|.
     std::vector<int64_t> stride(m.ns);
@@ -232,53 +521,122 @@ cufsp_status kron_create(const ModelHost &m, KronData **out) {
     for (int r = 0; r < m.nr; ++r) {
         int64_t d = 0;
         for (int s = 0; s < m.ns; ++s) d += (int64_t)m.nu[(size_t)r * m.ns + s] * stride[s];
-        if (d > m.n || d < -m.n) d = 0;  // such a neighbour is never inside the box
+        if (d > m.n || d < -m.n) d = 0;  // such a neighbour is never inside the box (factor 0)
         kd->delta[r] = (int)d;
         kd->halo = std::max<int64_t>(kd->halo, d < 0 ? -d : d);
     }
 
-    // Occupancy-derived persistent grid (computed for the V=1 kernel; refined below).
+    // Inner split (k species) and states per lane V: few idle lanes, large V.
     const DeviceInfo &di = device_info();
-    // Inner split: choose k (species 0..k-1 inner) to minimise idle lanes in the last chunk.
-    double best_waste = 1e30;
-    int best_k = 1;
+    int vmax = max_v_for(kd->NR);
+    if (const char *ev = getenv("CUFSP_KRON_VMAX")) {  // tuning override: cap states per lane (1, 2, 4)
+        const int v = atoi(ev);
+        if (v == 1 || v == 2 || v == 4) vmax = std::min(vmax, v);
+    }
+    double best = 1e300;
+    int best_k = 1, best_v = 1;
     int64_t Lk = 1;
     for (int k = 1; k <= m.ns; ++k) {
         Lk *= kd->dims[k - 1];
         if (Lk > 2147483647LL) break;
-        const int Vk = (Lk % 2 == 0 && kd->NR <= 8) ? 2 : 1;
-        const int64_t w = 32LL * Vk;
-        const int64_t chunks = (Lk + w - 1) / w;
-        if (chunks > (int64_t)di.sm_count * 16) break;  // keep at least ~4 rows of warps per sweep
-        const double waste = (double)(chunks * w - Lk) / (double)Lk;
-        if (waste < best_waste - 1e-12) {
-            best_waste = waste;
-            best_k = k;
+        for (int V = vmax; V >= 1; V /= 2) {
+            if (Lk % V) continue;
+            const int64_t w = 32LL * V;
+            const int64_t chunks = (Lk + w - 1) / w;
+            if (chunks > (int64_t)di.sm_count * 16 && !(k == 1 && V == 1)) continue;
+            const double waste = (double)(chunks * w - Lk) / (double)Lk;
+            const double score = (1.0 + waste) * (1.0 + 0.5 / V);
+            if (score < best - 1e-12) {
+                best = score;
+                best_k = k;
+                best_v = V;
+            }
         }
     }
     kd->k = best_k;
+    kd->V = best_v;
     int64_t L = 1;
     for (int s = 0; s < best_k; ++s) L *= kd->dims[s];
     kd->L = (int)L;
     kd->Q = (int)(m.n / L);
-    kd->V = (L % 2 == 0 && kd->NR <= 8) ? 2 : 1;
     kd->n_chunks = (int)((L + 32LL * kd->V - 1) / (32LL * kd->V));
+    // Rows q whose gathers stay in [0, n): q L >= max d_r and (q + 1) L <= n + min d_r.
+    int64_t dmax = 0, dmin = 0;
+    for (int r = 0; r < m.nr; ++r) {
+        dmax = std::max<int64_t>(dmax, kd->delta[r]);
+        dmin = std::min<int64_t>(dmin, kd->delta[r]);
+    }
+    kd->q_safe_lo = (int)((dmax + 1 + L - 1) / L);  // +1: odd shifts load the pair one element lower
+    kd->q_safe_hi = (int)std::max<int64_t>(0, (m.n + dmin) / L);
+    if (const char *ev = getenv("CUFSP_KRON_PF")) {  // tuning override: L2 prefetch distance in rows
+        const int v = atoi(ev);
+        if (v >= 0 && v <= 64) kd->pf_dist = v;
+    }
+
+    const std::vector<double2> g = outer_table(m, kd, best_k);
+
+    // Diagonal groups: reactions whose inner factor tables (species < k) are identical share one
+    // per-lane factor, so the diagonal costs one FMA per group and state instead of per reaction.
+    kd->gid.assign(CUFSP_MAX_REACTIONS, 0);
+    kd->rep.assign(CUFSP_MAX_REACTIONS, 0);
+    int ng = 0;
+    for (int r = 0; r < m.nr; ++r) {
+        int found = -1;
+        for (int gg = 0; gg < ng && found < 0; ++gg) {
+            const int r2 = kd->rep[gg];
+            bool same = true;
+            for (int s = 0; s < best_k && same; ++s) {
+                const double *a1 = m.tables.data() + (size_t)r * m.tab_stride + m.tab_off[s];
+                const double *a2 = m.tables.data() + (size_t)r2 * m.tab_stride + m.tab_off[s];
+                same = std::equal(a1, a1 + kd->dims[s], a2);
+            }
+            if (same) found = gg;
+        }
+        if (found < 0) {
+            found = ng;
+            kd->rep[ng++] = r;
+        }
+        kd->gid[r] = found;
+    }
+    kd->NG = (ng <= 2 && kd->NR > 2) ? 2 : (ng <= 4 && kd->NR > 4) ? 4 : kd->NR;
+    if (kd->NG == kd->NR) {  // no grouping: the diagonal keeps one term per reaction
+        for (int r = 0; r < CUFSP_MAX_REACTIONS; ++r) kd->gid[r] = kd->rep[r] = (r < kd->NR ? r : 0);
+    }
 
     int occ = 0;
-    KronKernel kern = pick_kernel(kd->NR, kd->V, true);
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, 256, 0);
+    KronKernel kern = pick_kernel(kd->NR, kd->NG, kd->V, true);
+    if (!kern) {
+        kron_destroy(kd);
+        return set_error(CUFSP_ERR_UNSUPPORTED, "no KRONECKER kernel for this reaction count");
+    }
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kKronThreads, 0);
     if (e != cudaSuccess || occ < 1) occ = 1;
     kd->grid_full = di.sm_count * occ;
 
-    const size_t tsz = (size_t)m.nr * m.tab_stride;
-    e = cudaMalloc(&kd->d_tables, sizeof(double) * tsz);
-    if (e == cudaSuccess) e = cudaMalloc(&kd->d_nu, sizeof(int) * m.nu.size());
-    if (e == cudaSuccess) e = cudaMemcpy(kd->d_tables, m.tables.data(), sizeof(double) * tsz, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(kd->d_nu, m.nu.data(), sizeof(int) * m.nu.size(), cudaMemcpyHostToDevice);
+    // Tables padded to NR reactions (padding rows are zero: no contribution, in-bounds reads).
+    std::vector<double> tabp((size_t)kd->NR * m.tab_stride, 0.0);
+    std::copy(m.tables.begin(), m.tables.end(), tabp.begin());
+    std::vector<int> nup((size_t)kd->NR * m.ns, 0);
+    std::copy(m.nu.begin(), m.nu.end(), nup.begin());
+    e = cudaMalloc(&kd->d_tables, sizeof(double) * tabp.size());
+    if (e == cudaSuccess) e = cudaMalloc(&kd->d_nu, sizeof(int) * nup.size());
+    if (e == cudaSuccess) e = cudaMalloc(&kd->d_gtab, sizeof(double2) * g.size());
+    if (e == cudaSuccess) e = cudaMemcpy(kd->d_tables, tabp.data(), sizeof(double) * tabp.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(kd->d_nu, nup.data(), sizeof(int) * nup.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(kd->d_gtab, g.data(), sizeof(double2) * g.size(), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
         kron_destroy(kd);
         return cuda_error(e, "kron_create");
     }
+    plan_march(m, kd);
+    if (kd->march && kd->ma.k != kd->k) {  // the marching split needs its own outer table
+        const std::vector<double2> gm = outer_table(m, kd, kd->ma.k);
+        e = cudaMalloc(&kd->d_gtab_march, sizeof(double2) * gm.size());
+        if (e == cudaSuccess)
+            e = cudaMemcpy(kd->d_gtab_march, gm.data(), sizeof(double2) * gm.size(), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) kd->march = false;
+    }
+    cudaGetLastError();  // a declined fast path leaves no sticky error behind
     *out = kd;
     return CUFSP_SUCCESS;
 }
@@ -287,7 +645,18 @@ void kron_destroy(KronData *k) {
     if (!k) return;
     if (k->d_tables) cudaFree(k->d_tables);
     if (k->d_nu) cudaFree(k->d_nu);
+    if (k->d_gtab) cudaFree(k->d_gtab);
+    if (k->d_gtab_march) cudaFree(k->d_gtab_march);
+    if (k->d_err) cudaFree(k->d_err);
     delete k;
+}
+
+int kron_watchdog(KronData *k) {
+    if (!k || !k->d_err) return 0;
+    int v = 0;
+    if (cudaMemcpy(&v, k->d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+    if (v) cudaMemset(k->d_err, 0, sizeof(int));
+    return v;
 }
 
 int64_t kron_halo(const KronData *k) { return k->halo; }
@@ -295,21 +664,46 @@ int64_t kron_row_len(const KronData *k) { return k->L; }
 
 cufsp_status kron_apply(KronData *kd, const double *coefs, double alpha, const double *d_alpha, const int *d_skip,
                         const double *x, bool accumulate, double *y, cudaStream_t st, int64_t i_begin, int64_t i_end) {
+    const bool full = i_begin == 0 && (i_end < 0 || i_end == kd->n);
+    if (kd->march && full && (reinterpret_cast<uintptr_t>(x) % 16) == 0) {
+        MarchArgs ma = kd->ma;
+        ma.gtab = kd->d_gtab_march ? kd->d_gtab_march : kd->d_gtab;
+        ma.tables = kd->d_tables;
+        ma.nu = kd->d_nu;
+        ma.d_alpha = d_alpha;
+        ma.d_skip = d_skip;
+        ma.err = kd->d_err;
+        for (int r = 0; r < CUFSP_MAX_REACTIONS; ++r) ma.coef[r] = r < kd->nr ? alpha * coefs[r] : 0.0;
+        MarchKernel mk = pick_march_kernel(kd->NR, kd->march_V, accumulate);
+        if (mk) {
+            mk<<<(unsigned)kd->march_grid, (unsigned)kd->march_threads, kd->march_smem, st>>>(ma, x, y);
+            CUFSP_CUDA_TRY(cudaGetLastError());
+            return CUFSP_SUCCESS;
+        }
+    }
     KronArgs a;
     a.tables = kd->d_tables;
     a.nu = kd->d_nu;
+    a.gtab = kd->d_gtab;
     a.d_alpha = d_alpha;
     a.d_skip = d_skip;
-    a.n = kd->n;
+    a.n = (int)kd->n;
     a.tab_stride = kd->tab_stride;
     a.ns = kd->ns;
     a.nr = kd->nr;
     a.k = kd->k;
     a.L = kd->L;
-    a.n_chunks = kd->n_chunks;
+    // V >= 2 moves x and y in 16-byte pairs; vectors only 8-byte aligned take the V = 1 kernel.
+    const bool aligned16 = ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) % 16) == 0;
+    const int V = aligned16 ? kd->V : 1;
+    const int n_chunks = (int)((kd->L + 32LL * V - 1) / (32LL * V));
+    a.n_chunks = n_chunks;
     if (i_end < 0) i_end = kd->n;
     a.q_begin = (int)(i_begin / kd->L);
     a.q_end = (int)((i_end + kd->L - 1) / kd->L);
+    a.q_safe_lo = kd->q_safe_lo;
+    a.q_safe_hi = kd->q_safe_hi;
+    a.pf_dist = V >= 2 ? kd->pf_dist : 0;  // the bulk L2 prefetch only pays off for paired loads
     for (int s = 0; s < CUFSP_MAX_SPECIES; ++s) {
         a.dims[s] = s < kd->ns ? kd->dims[s] : 1;
         a.tab_off[s] = s < kd->ns ? kd->tab_off[s] : 0;
@@ -317,18 +711,20 @@ cufsp_status kron_apply(KronData *kd, const double *coefs, double alpha, const d
     for (int r = 0; r < CUFSP_MAX_REACTIONS; ++r) {
         a.delta[r] = r < kd->nr ? kd->delta[r] : 0;
         a.coef[r] = r < kd->nr ? alpha * coefs[r] : 0.0;
+        a.gid[r] = kd->gid[r];
+        a.rep[r] = kd->rep[r];
     }
     const int rows = a.q_end - a.q_begin;
     if (rows <= 0) return CUFSP_SUCCESS;
     // Enough warps for every chunk, at most the persistent grid, and >= ~4 rows per warp.
-    int64_t want_warps = (int64_t)kd->n_chunks * ((rows + 3) / 4);
-    int64_t grid = (want_warps + 7) / 8;
-    int64_t min_grid = (kd->n_chunks + 7) / 8;
+    const int64_t min_grid = (n_chunks + kKronWarps - 1) / kKronWarps;
+    const int64_t want_warps = (int64_t)n_chunks * ((rows + 3) / 4);
+    int64_t grid = (want_warps + kKronWarps - 1) / kKronWarps;
     grid = std::max(grid, min_grid);
     grid = std::min<int64_t>(grid, std::max<int64_t>(kd->grid_full, min_grid));
-    KronKernel kern = pick_kernel(kd->NR, kd->V, accumulate);
+    KronKernel kern = pick_kernel(kd->NR, kd->NG, V, accumulate);
     if (!kern) return set_error(CUFSP_ERR_UNSUPPORTED, "no KRONECKER kernel for this reaction count");
-    kern<<<(unsigned)grid, 256, 0, st>>>(a, x, y);
+    kern<<<(unsigned)grid, kKronThreads, 0, st>>>(a, x, y);
     CUFSP_CUDA_TRY(cudaGetLastError());
     return CUFSP_SUCCESS;
 }

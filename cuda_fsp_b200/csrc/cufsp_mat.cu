@@ -99,6 +99,14 @@ extern "C" cufsp_status cufsp_mat_action(cufsp_mat *A, double t, const double *x
     return cufsp_mat_apply(A, t, nullptr, 1.0, x, 1.0, y, stream);
 }
 
+extern "C" cufsp_status cufsp_mat_watchdog(cufsp_mat *A, int *tripped) {
+    if (!A || !tripped) return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_mat_watchdog: NULL argument");
+    const int v = A->kron ? kron_watchdog(A->kron) : 0;
+    if (v < 0) return set_error(CUFSP_ERR_CUDA, "cufsp_mat_watchdog: device read failed");
+    *tripped = v;
+    return CUFSP_SUCCESS;
+}
+
 extern "C" cufsp_status cufsp_mat_export_propensities(const cufsp_mat *A, double *d_props, cufsp_stream_t stream) {
     if (!A || !d_props) return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_mat_export_propensities: NULL argument");
     if (!A->sparse) return set_error(CUFSP_ERR_UNSUPPORTED, "propensity export needs the CSR/HYB format");

@@ -169,6 +169,12 @@ class FSPMat:
         _lib.check(self._lib, self._lib.cufsp_mat_action_host(self._h, float(t), hp(x_host), hp(y_host)),
                    "cufsp_mat_action_host")
 
+    def watchdog(self) -> int:
+        """1 if a bounded barrier wait of the TMA-fed kernel expired since the last call."""
+        t = C.c_int()
+        _lib.check(self._lib, self._lib.cufsp_mat_watchdog(self._h, C.byref(t)), "cufsp_mat_watchdog")
+        return int(t.value)
+
     def export_propensities(self):
         import torch
         out = torch.empty((self.nr, self.n), dtype=torch.float64, device="cuda")

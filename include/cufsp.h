@@ -116,6 +116,11 @@ cufsp_status cufsp_mat_apply(cufsp_mat *A, double t, const double *coefs, double
  * x_host / y_host should be pinned (cudaHostAlloc) for full PCIe bandwidth. */
 cufsp_status cufsp_mat_action_host(cufsp_mat *A, double t, const double *x_host, double *y_host);
 
+/* Watchdog of the TMA-fed KRONECKER kernel: *tripped = 1 when one of its bounded shared-memory
+ * barrier waits expired since the previous call (the affected output is then incomplete); the flag
+ * is reset.  Synchronises the device. */
+cufsp_status cufsp_mat_watchdog(cufsp_mat *A, int *tripped);
+
 /* Sparse-format export for checking (HYB/CSR formats only): props[r*n + i] = a_r(x_i). */
 cufsp_status cufsp_mat_export_propensities(const cufsp_mat *A, double *d_props, cufsp_stream_t stream);
 

@@ -13,19 +13,19 @@ def dev(a):
     return torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device="cuda")
 
 
-def run_gpu(m, t_final, fmt=MatrixFormat.KRONECKER, **kw):
+def run_gpu(model, t_final, fmt=MatrixFormat.KRONECKER, **kw):
     import torch
-    A = FSPMat.from_model(m, fmt)
-    v = dev(m.p0())
-    E = KryExpvFSP(t_final, A, v, coefs=m.coefs(0), **kw)
+    A = FSPMat.from_model(model, fmt)
+    v = dev(model.p0())
+    E = KryExpvFSP(t_final, A, v, coefs=model.coefs(0), **kw)
     st = E.solve()
     torch.cuda.synchronize()
     return v.cpu().numpy(), st
 
 
-def run_oracle(m, t_final, **kw):
-    csr = oracle.assemble_model(m)
-    w, st, rc = oracle.expv(csr, m.coefs(0), t_final, m.p0(), **kw)
+def run_oracle(model, t_final, **kw):
+    csr = oracle.assemble_model(model)
+    w, st, rc = oracle.expv(csr, model.coefs(0), t_final, model.p0(), **kw)
     assert rc == 0
     return w, st
 
@@ -52,15 +52,27 @@ def test_reference_mass_conservation_case(cuda):
     |1 - sum v| <= 1e-10."""
     import torch
     m = models.toggle((256, 256))
+    T = 8 * 3600.0
+    # Expokit's tol bounds the local error per unit time, so over t = 28,800 the global error of
+    # either implementation is ~1e-5; both are compared with a tol = 1e-13 oracle solution.
+    # The realised error of either implementation moves between ~1e-7 and ~1e-5 with rounding
+    # (it changes the accepted step sizes), so the bar is the method's own budget delta*tol*T.
+    truth, _ = run_oracle(m, T, m=40, tol=1e-13)
+    budget = 1.2 * 1e-8 * T
+    w_orc, _ = run_oracle(m, T, m=30, tol=1e-8, iop=True, q_iop=2)
+    assert np.abs(w_orc - truth).sum() <= budget
     for fmt in (MatrixFormat.HYB, MatrixFormat.KRONECKER):
-        w, st = run_gpu(m, 8 * 3600.0, fmt, m=30, tol=1e-8, iop=True, q_iop=2)
+        w, st = run_gpu(m, T, fmt, m=30, tol=1e-8, iop=True, q_iop=2)
         assert abs(1.0 - w.sum()) <= 1e-10
-    w_orc, _ = run_oracle(m, 8 * 3600.0, m=30, tol=1e-8, iop=True, q_iop=2)
-    assert np.abs(w - w_orc).sum() <= 1e-8
+        assert np.abs(w - truth).sum() <= budget
+    w_full, _ = run_gpu(m, T, MatrixFormat.KRONECKER, m=40, tol=1e-12)
+    assert np.abs(w_full - truth).sum() <= 1e-9
 
 
 def test_callback_matvec_equals_generator_path(cuda):
-    """The MVFun form (a callback accumulating A x into a zeroed y) gives the same result."""
+    """The MVFun form (a callback accumulating A x into a zeroed y, then scaled) agrees within the
+    Krylov tolerance: it rounds differently from the fused scaled action, and the adaptive step
+    control may then take a different step sequence."""
     import torch
     m = models.birth_death_2()
     A = FSPMat.from_model(m, MatrixFormat.KRONECKER)
@@ -74,7 +86,7 @@ def test_callback_matvec_equals_generator_path(cuda):
     v2 = dev(m.p0())
     KryExpvFSP(10.0, mv, v2, m=30).solve()
     torch.cuda.synchronize()
-    assert (v1 - v2).abs().sum().item() <= 1e-12
+    assert (v1 - v2).abs().sum().item() <= 1e-8
 
 
 def test_happy_breakdown(cuda):
