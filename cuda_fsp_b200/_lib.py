@@ -91,6 +91,7 @@ SIGNATURES = {
     "cufsp_expv_get_stats": [_P, C.POINTER(ExpvStats)],
     "cufsp_expm_host": [C.c_int, _DP, _DP],
     "cufsp_vec_sum": [C.c_int64, _P, _DP, _P],
+    "cufsp_vec_sum_noalloc": [C.c_int64, _P, _P, _P],
 }
 _RESTYPE = {"cufsp_status_string": C.c_char_p, "cufsp_last_error": C.c_char_p}
 

@@ -170,6 +170,21 @@ cufsp_status cufsp_expm_host(int k, const double *A, double *F);
 /* sum of x (deterministic order); result written to host *out; synchronises `stream`. */
 cufsp_status cufsp_vec_sum(int64_t n, const double *x, double *out, cufsp_stream_t stream);
 
+/* Sum of the n doubles at x (device), written to the device double *d_out, with NO device memory
+ * allocated: no counterpart in the reference.  It is meant for callers that cannot call cudaMalloc
+ * themselves or let a library do it -- a framework or serving runtime that owns all device memory
+ * through its own pool and accounts for every byte, or a code path that must not take the device
+ * synchronisation that cudaMalloc/cudaFree can imply.
+ * Limits and sharing: the scratch is a fixed 8 KB __device__ array in this library (one partial sum
+ * per 4096-element block), held on every GPU that loads the library until the process exits, so
+ * n <= CUFSP_NOALLOC_MAX_N; larger n returns CUFSP_ERR_INVALID_ARG.  The first call on a device looks
+ * the array's address up (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture.  All calls share the array: calls that overlap on the GPU (other
+ * streams, other host threads) race and must be serialised.  Asynchronous on `stream`; the
+ * summation order is fixed, so the result is reproducible. */
+#define CUFSP_NOALLOC_MAX_N 4194304
+cufsp_status cufsp_vec_sum_noalloc(int64_t n, const double *x, double *d_out, cufsp_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif
