@@ -25,7 +25,7 @@ LIB = PKG / "lib"
 OBJ = PKG / "_build"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-rdc=true", "-Xcompiler", "-fPIC,-O2",
-                     "-I" + str(ROOT / "include"), "--expt-relaxed-constexpr"]
+                     "-I" + str(ROOT / "include"), "--expt-relaxed-constexpr", "--extended-lambda"]
 SOURCES = ["cufsp_common.cu", "cufsp_kron.cu", "cufsp_kron_march.cu", "cufsp_sparse.cu", "cufsp_mat.cu",
            "cufsp_krylov.cu", "cufsp_expm.cpp", "cufsp_noalloc.cu"]
 HEADERS = ["cufsp_internal.h", "cufsp_reduce.cuh", "cufsp_march.h"]
