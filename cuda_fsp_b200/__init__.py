@@ -7,5 +7,7 @@ definitions in `models`.
 from . import models
 from ._lib import CufspError
 from .fsp import FSPMat, KryExpvFSP, MatrixFormat, expm, get_states, num_states
+from .likelihood import FSPSolver, Likelihood, generate_data, histograms
 
-__all__ = ["models", "CufspError", "FSPMat", "KryExpvFSP", "MatrixFormat", "expm", "get_states", "num_states"]
+__all__ = ["models", "CufspError", "FSPMat", "KryExpvFSP", "MatrixFormat", "expm", "get_states", "num_states",
+           "FSPSolver", "Likelihood", "generate_data", "histograms"]

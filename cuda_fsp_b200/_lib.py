@@ -55,6 +55,14 @@ class ExpvStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class SolverStatus(C.Structure):
+    _fields_ = [("time_index", C.c_int), ("t", C.c_double), ("fsp_error", C.c_double), ("fsp_tol_exceeded", C.c_int),
+                ("krylov_steps", C.c_int64), ("matvecs", C.c_int64)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 _P = C.c_void_p
 _I64P = C.POINTER(C.c_int64)
 _IP = C.POINTER(C.c_int)
@@ -90,6 +98,14 @@ SIGNATURES = {
     "cufsp_expv_final_time_reached": [_P, _IP],
     "cufsp_expv_get_stats": [_P, C.POINTER(ExpvStats)],
     "cufsp_expm_host": [C.c_int, _DP, _DP],
+    "cufsp_solver_create": [_P, _DP, C.c_int, C.c_double, _DP, C.c_double, C.c_int, C.c_int, C.c_int, C.POINTER(_P)],
+    "cufsp_solver_destroy": [_P],
+    "cufsp_solver_set_coefs": [_P, _DP],
+    "cufsp_solver_next_time": [_P, _P, _P, C.POINTER(SolverStatus)],
+    "cufsp_solver_solve": [_P, _P, _P, C.POINTER(SolverStatus)],
+    "cufsp_solver_reset_time": [_P],
+    "cufsp_loglik": [C.c_int64, _P, C.c_int64, _P, _DP, _P],
+    "cufsp_ssa": [C.POINTER(ModelDesc), _DP, _IP, _DP, C.c_int, C.c_int, C.c_ulonglong, C.c_int64, _P, _P],
     "cufsp_vec_sum": [C.c_int64, _P, _DP, _P],
     "cufsp_vec_sum_noalloc": [C.c_int64, _P, _P, _P],
 }

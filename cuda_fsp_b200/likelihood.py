@@ -1,0 +1,155 @@
+"""Python mirror of the reference's solver / statistics API (cme namespace, never compiled there).
+
+  FSPSolver      <- cme::FSPSolver   (src/FSPSolver.h:16-111)
+  Likelihood     <- cme::Likelihood  (src/Likelihood.h:20-57, src/Likelihood.cpp:8-33)
+  generate_data  <- cme::generate_data (src/Likelihood.cpp:35-84), seeded
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import _lib
+from ._lib import ModelDesc, SolverStatus
+from .fsp import FSPMat, MatrixFormat, _ptr, _stream
+
+
+class FSPSolver:
+    """Advances a device probability vector through output times; reports the FSP error
+    sum(p(0)) - sum(p(t)) against fsp_tol after every advance."""
+
+    def __init__(self, A: FSPMat, p, times, fsp_tol: float = 1e-4, kry_tol: float = 1e-8, m: int = 30,
+                 iop: bool = False, q_iop: int = 2, coefs=None):
+        self._lib = A._lib
+        self.A, self.p = A, p
+        self.times = np.ascontiguousarray(np.asarray(times, np.float64))
+        cp = None
+        if coefs is not None:
+            self._coefs = np.ascontiguousarray(np.asarray(coefs, np.float64))
+            cp = self._coefs.ctypes.data_as(C.POINTER(C.c_double))
+        self._h = C.c_void_p()
+        _lib.check(self._lib, self._lib.cufsp_solver_create(
+            A.handle, self.times.ctypes.data_as(C.POINTER(C.c_double)), len(self.times), float(fsp_tol), cp,
+            float(kry_tol), int(m), int(bool(iop)), int(q_iop), C.byref(self._h)), "cufsp_solver_create")
+        self.status: dict | None = None
+
+    def set_coefs(self, coefs) -> None:
+        self._coefs = np.ascontiguousarray(np.asarray(coefs, np.float64))
+        _lib.check(self._lib, self._lib.cufsp_solver_set_coefs(self._h, self._coefs.ctypes.data_as(C.POINTER(C.c_double))),
+                   "cufsp_solver_set_coefs")
+
+    def next_time(self, stream=None) -> dict:
+        st = SolverStatus()
+        _lib.check(self._lib, self._lib.cufsp_solver_next_time(self._h, _ptr(self.p), _stream(stream), C.byref(st)),
+                   "cufsp_solver_next_time")
+        self.status = st.as_dict()
+        return self.status
+
+    def solve(self, stream=None) -> dict:
+        st = SolverStatus()
+        _lib.check(self._lib, self._lib.cufsp_solver_solve(self._h, _ptr(self.p), _stream(stream), C.byref(st)),
+                   "cufsp_solver_solve")
+        self.status = st.as_dict()
+        return self.status
+
+    def reset_time(self) -> None:
+        _lib.check(self._lib, self._lib.cufsp_solver_reset_time(self._h), "cufsp_solver_reset_time")
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            self._lib.cufsp_solver_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def generate_data(model, times, x0, n_cells: int, seed: int = 20261203, coefs=None, max_events: int = 10**8,
+                  lib=None) -> np.ndarray:
+    """Seeded SSA snapshots: int32 array [n_times, n_cells, n_species], an independent trajectory
+    per (time, cell)."""
+    import torch
+    lib = lib or _lib.load()
+    b = np.ascontiguousarray(np.asarray(model.bounds, np.int32))
+    sv, sc, sr = model.stoich_csr()
+    tab = np.ascontiguousarray(model.tables, np.float64)
+    d = ModelDesc()
+    d.n_species, d.n_reactions = model.ns, model.nr
+    d.fsp_bounds = b.ctypes.data_as(C.POINTER(C.c_int))
+    d.stoich_vals = sv.ctypes.data_as(C.POINTER(C.c_int))
+    d.stoich_colidxs = sc.ctypes.data_as(C.POINTER(C.c_int))
+    d.stoich_rowptrs = sr.ctypes.data_as(C.POINTER(C.c_int))
+    d.factor_tables = tab.ctypes.data_as(C.POINTER(C.c_double))
+    c = np.ascontiguousarray(np.asarray(model.coefs(0.0) if coefs is None else coefs, np.float64))
+    x0a = np.ascontiguousarray(np.asarray(x0, np.int32))
+    t = np.ascontiguousarray(np.asarray(times, np.float64))
+    out = torch.empty((len(t), n_cells, model.ns), dtype=torch.int32, device="cuda")
+    _lib.check(lib, lib.cufsp_ssa(C.byref(d), c.ctypes.data_as(C.POINTER(C.c_double)),
+                                  x0a.ctypes.data_as(C.POINTER(C.c_int)), t.ctypes.data_as(C.POINTER(C.c_double)),
+                                  len(t), int(n_cells), C.c_ulonglong(seed), int(max_events), out.data_ptr(),
+                                  _stream(None)), "cufsp_ssa")
+    return out.cpu().numpy()
+
+
+def histograms(snapshots: np.ndarray, bounds, n_marginal: int = 0):
+    """Counts per time over the species n_marginal.. (the fastest n_marginal are summed out):
+    returns (counts [n_times, prod(kept b+1)] float64, outside [n_times] cells outside the box)."""
+    bounds = np.asarray(bounds)
+    kept = bounds[n_marginal:]
+    nk = int(np.prod(kept + 1))
+    T = snapshots.shape[0]
+    counts = np.zeros((T, nk))
+    outside = np.zeros(T, np.int64)
+    for it in range(T):
+        x = snapshots[it][:, n_marginal:]
+        inside = np.all((x >= 0) & (x <= kept), axis=1)
+        outside[it] = int((~inside).sum())
+        idx = np.zeros(int(inside.sum()), np.int64)
+        stride = 1
+        for s in range(len(kept)):
+            idx += x[inside, s].astype(np.int64) * stride
+            stride *= int(kept[s]) + 1
+        counts[it] = np.bincount(idx, minlength=nk)
+    return counts, outside
+
+
+class Likelihood:
+    """log L(theta) = sum_t sum_cells log max(1e-44, p_t(cell)) with p_t from the FSP solution at the
+    data times, marginalised over the n_marginal fastest species (src/Likelihood.cpp:8-33).  Cells
+    outside the FSP box contribute log(1e-44).  `evaluate(coefs)` takes the reaction coefficients."""
+
+    def __init__(self, model, times, counts, outside=None, n_marginal: int = 0, fsp_tol: float = 1e-4,
+                 kry_tol: float = 1e-8, m: int = 30, fmt: MatrixFormat = MatrixFormat.KRONECKER, lib=None):
+        import torch
+        self.model = model
+        self.times = np.asarray(times, np.float64)
+        self.block = int(np.prod(np.asarray(model.bounds[:n_marginal]) + 1)) if n_marginal else 1
+        self.A = FSPMat.from_model(model, fmt, lib=lib)
+        self.counts = torch.as_tensor(np.ascontiguousarray(counts, np.float64), device="cuda")
+        assert self.counts.shape == (len(self.times), model.n_states // self.block)
+        self.outside = np.zeros(len(self.times)) if outside is None else np.asarray(outside, np.float64)
+        self.p0 = torch.as_tensor(model.p0(), device="cuda")
+        self.p = self.p0.clone()
+        self.solver = FSPSolver(self.A, self.p, self.times, fsp_tol, kry_tol, m, coefs=model.coefs(0.0))
+        self.fsp_errors: list[float] = []
+
+    def evaluate(self, coefs=None) -> float:
+        if coefs is not None:
+            self.solver.set_coefs(coefs)
+        self.p.copy_(self.p0)  # return the distribution to the initial condition (:24-30)
+        self.solver.reset_time()
+        lib, n = self.A._lib, self.model.n_states
+        ll, self.fsp_errors = 0.0, []
+        for it in range(len(self.times)):
+            st = self.solver.next_time()
+            self.fsp_errors.append(st["fsp_error"])
+            out = C.c_double()
+            _lib.check(lib, lib.cufsp_loglik(n, self.p.data_ptr(), self.block, self.counts[it].data_ptr(),
+                                             C.byref(out), _stream(None)), "cufsp_loglik")
+            ll += out.value + self.outside[it] * math.log(1e-44)
+        return ll

@@ -162,6 +162,49 @@ cufsp_status cufsp_expv_reset_time(cufsp_expv *E);
 cufsp_status cufsp_expv_final_time_reached(const cufsp_expv *E, int *reached);
 cufsp_status cufsp_expv_get_stats(const cufsp_expv *E, cufsp_expv_stats *stats);
 
+/* ---- FSP solver through output times ------------------------------------------------------
+ * Replaces cme::FSPSolver (src/FSPSolver.h:16-111, src/FSPSolver.cpp:9-22; never compiled in the
+ * reference, semantics defined here): next_time() advances the caller's device vector p from the
+ * current time to the next output time with the Krylov exponential of the time-invariant
+ * generator (coefs: host, n_reactions doubles, or NULL for tcoef(0)); solve() goes to the last
+ * time; reset_time() returns to t = 0 keeping the vector.  After each advance the FSP truncation
+ * error sum(p(0)) - sum(p(t)) is reported and compared with fsp_tol (stored, unused, in the
+ * reference: FSPSolver.h:28).  Synchronous. */
+typedef struct {
+    int time_index;       /* index of the output time reached */
+    double t;             /* time reached */
+    double fsp_error;     /* probability that left the FSP box so far */
+    int fsp_tol_exceeded; /* fsp_error > fsp_tol */
+    int64_t krylov_steps; /* cumulative Krylov steps */
+    int64_t matvecs;      /* cumulative generator applications */
+} cufsp_solver_status;
+typedef struct cufsp_solver_s cufsp_solver;
+cufsp_status cufsp_solver_create(cufsp_mat *A, const double *times, int n_times, double fsp_tol,
+                                 const double *coefs, double kry_tol, int m, int iop, int q_iop,
+                                 cufsp_solver **out);
+cufsp_status cufsp_solver_destroy(cufsp_solver *S);
+cufsp_status cufsp_solver_set_coefs(cufsp_solver *S, const double *coefs);
+cufsp_status cufsp_solver_next_time(cufsp_solver *S, double *d_p, cufsp_stream_t stream, cufsp_solver_status *status);
+cufsp_status cufsp_solver_solve(cufsp_solver *S, double *d_p, cufsp_stream_t stream, cufsp_solver_status *status);
+cufsp_status cufsp_solver_reset_time(cufsp_solver *S);
+
+/* ---- likelihood and data generation ----------------------------------------------------------
+ * One time point of Likelihood::evaluate (src/Likelihood.cpp:14-21):
+ *   *out = sum_k counts[k] * log(max(1e-44, q[k])),  q[k] = sum_{j<block} p[k*block + j],
+ * i.e. p marginalised over the fastest-varying species whose index range has `block` states
+ * (block = 1: no marginalisation).  d_p, d_counts: device, n and n/block doubles.  Synchronous. */
+cufsp_status cufsp_loglik(int64_t n, const double *d_p, int64_t block, const double *d_counts, double *out,
+                          cufsp_stream_t stream);
+/* generate_data (src/Likelihood.cpp:35-84): Gillespie direct method from x0 (host, n_species
+ * ints), an independent trajectory per (time, cell) as single-cell snapshots are, Philox streams
+ * seeded by `seed`.  Propensities c_r * prod_s f_{r,s}(x_s) from the model's factor tables
+ * (counts beyond the box use the table's edge value); coefs: host, or NULL for tcoef(0).
+ * d_out: device int[n_times][n_cells][n_species].  CUFSP_ERR_STEP_LIMIT when a trajectory needs
+ * more than max_events reactions.  Synchronous. */
+cufsp_status cufsp_ssa(const cufsp_model_desc *desc, const double *coefs, const int *x0, const double *times,
+                       int n_times, int n_cells, unsigned long long seed, int64_t max_events, int *d_out,
+                       cufsp_stream_t stream);
+
 /* Dense exponential of a k x k column-major host matrix by scaling-and-squaring Pade(13,13)
  * (replaces arma::expmat at src/KryExpvFSP.cu:125). */
 cufsp_status cufsp_expm_host(int k, const double *A, double *F);
