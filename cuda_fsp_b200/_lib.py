@@ -63,6 +63,15 @@ class SolverStatus(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class BdfStats(C.Structure):
+    _fields_ = [("t", C.c_double), ("h", C.c_double), ("last_err", C.c_double), ("order", C.c_int),
+                ("pad", C.c_int), ("n_steps", C.c_int64), ("n_reject", C.c_int64), ("n_matvec", C.c_int64),
+                ("n_lin_iters", C.c_int64), ("n_lin_fail", C.c_int64)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}
+
+
 _P = C.c_void_p
 _I64P = C.POINTER(C.c_int64)
 _IP = C.POINTER(C.c_int)
@@ -98,7 +107,15 @@ SIGNATURES = {
     "cufsp_expv_final_time_reached": [_P, _IP],
     "cufsp_expv_get_stats": [_P, C.POINTER(ExpvStats)],
     "cufsp_expm_host": [C.c_int, _DP, _DP],
+    "cufsp_bdf_create": [_P, _DP, C.c_double, C.c_double, C.c_int, C.POINTER(_P)],
+    "cufsp_bdf_destroy": [_P],
+    "cufsp_bdf_set_options": [_P, C.c_double, C.c_double, C.c_double, C.c_int64],
+    "cufsp_bdf_set_coefs": [_P, _DP],
+    "cufsp_bdf_init": [_P, C.c_double, _P, _P],
+    "cufsp_bdf_advance": [_P, C.c_double, _P, C.c_int, _P, _DP],
+    "cufsp_bdf_get_stats": [_P, C.POINTER(BdfStats)],
     "cufsp_solver_create": [_P, _DP, C.c_int, C.c_double, _DP, C.c_double, C.c_int, C.c_int, C.c_int, C.POINTER(_P)],
+    "cufsp_solver_create_bdf": [_P, _DP, C.c_int, C.c_double, _DP, C.c_double, C.c_double, C.POINTER(_P)],
     "cufsp_solver_destroy": [_P],
     "cufsp_solver_set_coefs": [_P, _DP],
     "cufsp_solver_next_time": [_P, _P, _P, C.POINTER(SolverStatus)],

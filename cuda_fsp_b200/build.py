@@ -27,8 +27,9 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-rdc=true", "-Xcompiler", "-fPIC,-O2",
                      "-I" + str(ROOT / "include"), "--expt-relaxed-constexpr", "--extended-lambda"]
 SOURCES = ["cufsp_common.cu", "cufsp_kron.cu", "cufsp_kron_march.cu", "cufsp_sparse.cu", "cufsp_mat.cu",
-           "cufsp_krylov.cu", "cufsp_expm.cpp", "cufsp_noalloc.cu", "cufsp_stats.cu", "cufsp_solver.cu"]
-HEADERS = ["cufsp_internal.h", "cufsp_reduce.cuh", "cufsp_march.h"]
+           "cufsp_krylov.cu", "cufsp_expm.cpp", "cufsp_noalloc.cu", "cufsp_stats.cu", "cufsp_solver.cu",
+           "cufsp_vec.cu", "cufsp_bdf.cu"]
+HEADERS = ["cufsp_internal.h", "cufsp_reduce.cuh", "cufsp_march.h", "cufsp_vec.h"]
 
 
 def nvcc() -> str:

@@ -6,8 +6,10 @@
 // reset_time() returns to t = 0 (the vector is kept, as in the reference).  After every advance
 // the FSP truncation error 1 - sum(p) -- the probability that left the box through the generator's
 // boundary outflow -- is computed on the device and compared with fsp_tol (stored but unused by
-// the reference, FSPSolver.h:28).  Time-invariant generators use the Krylov exponential; the
-// coefficients c_r are taken at t = 0 or given explicitly.
+// the reference, FSPSolver.h:28).  Time-invariant generators use the Krylov exponential (the
+// coefficients c_r are taken at t = 0 or given explicitly); solvers made by
+// cufsp_solver_create_bdf integrate with the BDF method instead, which also handles c_r(t), and
+// read the caller's vector only at the first advance after create / reset_time / set_coefs.
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -19,6 +21,8 @@ using namespace cufsp;
 struct cufsp_solver_s {
     cufsp_mat *A = nullptr;
     cufsp_expv *E = nullptr;
+    cufsp_bdf *B = nullptr;  // BDF path (time-varying rates); E is then unused
+    bool bdf_ready = false;
     std::vector<double> times;
     double fsp_tol = 0.0;
     double t_now = 0.0;
@@ -49,7 +53,18 @@ cufsp_status advance_to(cufsp_solver *S, double t_target, double *d_p, cudaStrea
         S->have_mass0 = true;
     }
     const double dt = t_target - S->t_now;
-    if (dt > 0.0) {
+    if (S->B) {
+        if (!S->bdf_ready) {
+            cufsp_status s = cufsp_bdf_init(S->B, S->t_now, d_p, (cufsp_stream_t)st);
+            if (s != CUFSP_SUCCESS) return s;
+            S->bdf_ready = true;
+        }
+        cufsp_status s = cufsp_bdf_advance(S->B, t_target, d_p, 0, (cufsp_stream_t)st, nullptr);
+        if (s != CUFSP_SUCCESS) {
+            S->bdf_ready = false;
+            return s;
+        }
+    } else if (dt > 0.0) {
         cufsp_status s = cufsp_expv_set_final_time(S->E, dt);
         if (s == CUFSP_SUCCESS) s = cufsp_expv_reset_time(S->E);
         if (s == CUFSP_SUCCESS) s = cufsp_expv_solve(S->E, d_p, (cufsp_stream_t)st, nullptr);
@@ -59,22 +74,29 @@ cufsp_status advance_to(cufsp_solver *S, double t_target, double *d_p, cudaStrea
     double m = 0.0;
     cufsp_status s = mass(S, d_p, st, &m);
     if (s != CUFSP_SUCCESS) return s;
-    cufsp_expv_stats es;
-    cufsp_expv_get_stats(S->E, &es);
     S->last.t = S->t_now;
     S->last.time_index = S->index;
     S->last.fsp_error = S->mass0 - m;
     S->last.fsp_tol_exceeded = S->last.fsp_error > S->fsp_tol;
-    S->last.krylov_steps = es.n_steps;
-    S->last.matvecs = es.n_matvec;
+    if (S->B) {
+        cufsp_bdf_stats bs;
+        cufsp_bdf_get_stats(S->B, &bs);
+        S->last.krylov_steps = bs.n_steps;
+        S->last.matvecs = bs.n_matvec;
+    } else {
+        cufsp_expv_stats es;
+        cufsp_expv_get_stats(S->E, &es);
+        S->last.krylov_steps = es.n_steps;
+        S->last.matvecs = es.n_matvec;
+    }
     return CUFSP_SUCCESS;
 }
 
 }  // namespace
 
-extern "C" cufsp_status cufsp_solver_create(cufsp_mat *A, const double *times, int n_times, double fsp_tol,
-                                            const double *coefs, double kry_tol, int m, int iop, int q_iop,
-                                            cufsp_solver **out) {
+namespace {
+
+cufsp_status solver_new(cufsp_mat *A, const double *times, int n_times, double fsp_tol, cufsp_solver **out) {
     clear_error();
     if (!out || !A || !times || n_times < 1 || !(fsp_tol >= 0.0))
         return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_solver_create: bad argument");
@@ -83,29 +105,56 @@ extern "C" cufsp_status cufsp_solver_create(cufsp_mat *A, const double *times, i
         if (!std::isfinite(times[i]) || times[i] < 0.0 || (i && !(times[i] > times[i - 1])))
             return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_solver_create: times must be finite, >= 0, increasing");
     }
-    int64_t n = 0;
-    cufsp_mat_num_states(A, &n);
     cufsp_solver *S = new cufsp_solver();
     S->A = A;
     S->times.assign(times, times + n_times);
     S->fsp_tol = fsp_tol;
     std::memset(&S->last, 0, sizeof(S->last));
-    cufsp_status s = cufsp_expv_create(n, m, kry_tol, iop, q_iop, 1.0, &S->E);
-    if (s == CUFSP_SUCCESS) s = coefs ? cufsp_expv_bind_mat_coefs(S->E, A, coefs) : cufsp_expv_bind_mat(S->E, A, 0.0);
+    *out = S;
+    return CUFSP_SUCCESS;
+}
+
+cufsp_status solver_finish(cufsp_solver *S, cufsp_status s, cufsp_solver **out) {
     if (s == CUFSP_SUCCESS) s = S->rs.init(device_info().sm_count * 4, 1);
     if (s == CUFSP_SUCCESS && cudaMalloc(&S->d_sum, sizeof(double)) != cudaSuccess)
         s = set_error(CUFSP_ERR_ALLOC, "cufsp_solver_create: cudaMalloc");
     if (s != CUFSP_SUCCESS) {
         cufsp_solver_destroy(S);
+        *out = nullptr;
         return s;
     }
     *out = S;
     return CUFSP_SUCCESS;
 }
 
+}  // namespace
+
+extern "C" cufsp_status cufsp_solver_create_bdf(cufsp_mat *A, const double *times, int n_times, double fsp_tol,
+                                                const double *coefs, double rtol, double atol, cufsp_solver **out) {
+    cufsp_solver *S = nullptr;
+    cufsp_status s = solver_new(A, times, n_times, fsp_tol, &S);
+    if (s != CUFSP_SUCCESS) return s;
+    s = cufsp_bdf_create(A, coefs, rtol, atol, 30, &S->B);
+    return solver_finish(S, s, out);
+}
+
+extern "C" cufsp_status cufsp_solver_create(cufsp_mat *A, const double *times, int n_times, double fsp_tol,
+                                            const double *coefs, double kry_tol, int m, int iop, int q_iop,
+                                            cufsp_solver **out) {
+    cufsp_solver *S = nullptr;
+    cufsp_status s = solver_new(A, times, n_times, fsp_tol, &S);
+    if (s != CUFSP_SUCCESS) return s;
+    int64_t n = 0;
+    cufsp_mat_num_states(A, &n);
+    s = cufsp_expv_create(n, m, kry_tol, iop, q_iop, 1.0, &S->E);
+    if (s == CUFSP_SUCCESS) s = coefs ? cufsp_expv_bind_mat_coefs(S->E, A, coefs) : cufsp_expv_bind_mat(S->E, A, 0.0);
+    return solver_finish(S, s, out);
+}
+
 extern "C" cufsp_status cufsp_solver_destroy(cufsp_solver *S) {
     if (!S) return CUFSP_SUCCESS;
     cufsp_expv_destroy(S->E);
+    cufsp_bdf_destroy(S->B);
     if (S->d_sum) cudaFree(S->d_sum);
     S->rs.release();
     delete S;
@@ -113,7 +162,12 @@ extern "C" cufsp_status cufsp_solver_destroy(cufsp_solver *S) {
 }
 
 extern "C" cufsp_status cufsp_solver_set_coefs(cufsp_solver *S, const double *coefs) {
-    if (!S || !coefs) return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_solver_set_coefs: NULL argument");
+    if (!S) return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_solver_set_coefs: NULL argument");
+    if (S->B) {
+        S->bdf_ready = false;
+        return cufsp_bdf_set_coefs(S->B, coefs);
+    }
+    if (!coefs) return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_solver_set_coefs: NULL argument");
     return cufsp_expv_bind_mat_coefs(S->E, S->A, coefs);
 }
 
@@ -148,5 +202,6 @@ extern "C" cufsp_status cufsp_solver_reset_time(cufsp_solver *S) {
     S->index = 0;
     S->t_now = 0.0;
     S->have_mass0 = false;
+    S->bdf_ready = false;
     return CUFSP_SUCCESS;
 }

@@ -18,27 +18,41 @@ from .fsp import FSPMat, MatrixFormat, _ptr, _stream
 
 class FSPSolver:
     """Advances a device probability vector through output times; reports the FSP error
-    sum(p(0)) - sum(p(t)) against fsp_tol after every advance."""
+    sum(p(0)) - sum(p(t)) against fsp_tol after every advance.  method="krylov" uses the Krylov
+    exponential of the time-invariant generator; method="bdf" the BDF integrator (rtol, atol),
+    which with coefs=None follows the generator's c_r(t)."""
 
     def __init__(self, A: FSPMat, p, times, fsp_tol: float = 1e-4, kry_tol: float = 1e-8, m: int = 30,
-                 iop: bool = False, q_iop: int = 2, coefs=None):
+                 iop: bool = False, q_iop: int = 2, coefs=None, method: str = "krylov", rtol: float = 1e-8,
+                 atol: float = 1e-12):
         self._lib = A._lib
         self.A, self.p = A, p
+        self.method = method
         self.times = np.ascontiguousarray(np.asarray(times, np.float64))
         cp = None
         if coefs is not None:
             self._coefs = np.ascontiguousarray(np.asarray(coefs, np.float64))
             cp = self._coefs.ctypes.data_as(C.POINTER(C.c_double))
         self._h = C.c_void_p()
-        _lib.check(self._lib, self._lib.cufsp_solver_create(
-            A.handle, self.times.ctypes.data_as(C.POINTER(C.c_double)), len(self.times), float(fsp_tol), cp,
-            float(kry_tol), int(m), int(bool(iop)), int(q_iop), C.byref(self._h)), "cufsp_solver_create")
+        tp = self.times.ctypes.data_as(C.POINTER(C.c_double))
+        if method == "bdf":
+            _lib.check(self._lib, self._lib.cufsp_solver_create_bdf(
+                A.handle, tp, len(self.times), float(fsp_tol), cp, float(rtol), float(atol), C.byref(self._h)),
+                "cufsp_solver_create_bdf")
+        elif method == "krylov":
+            _lib.check(self._lib, self._lib.cufsp_solver_create(
+                A.handle, tp, len(self.times), float(fsp_tol), cp, float(kry_tol), int(m), int(bool(iop)), int(q_iop),
+                C.byref(self._h)), "cufsp_solver_create")
+        else:
+            raise ValueError(f"unknown method {method!r}")
         self.status: dict | None = None
 
     def set_coefs(self, coefs) -> None:
-        self._coefs = np.ascontiguousarray(np.asarray(coefs, np.float64))
-        _lib.check(self._lib, self._lib.cufsp_solver_set_coefs(self._h, self._coefs.ctypes.data_as(C.POINTER(C.c_double))),
-                   "cufsp_solver_set_coefs")
+        cp = None
+        if coefs is not None:
+            self._coefs = np.ascontiguousarray(np.asarray(coefs, np.float64))
+            cp = self._coefs.ctypes.data_as(C.POINTER(C.c_double))
+        _lib.check(self._lib, self._lib.cufsp_solver_set_coefs(self._h, cp), "cufsp_solver_set_coefs")
 
     def next_time(self, stream=None) -> dict:
         st = SolverStatus()

@@ -162,6 +162,48 @@ cufsp_status cufsp_expv_reset_time(cufsp_expv *E);
 cufsp_status cufsp_expv_final_time_reached(const cufsp_expv *E, int *reached);
 cufsp_status cufsp_expv_get_stats(const cufsp_expv *E, cufsp_expv_stats *stats);
 
+/* ---- BDF integrator for time-varying generators ------------------------------------------
+ * Replaces the SUNDIALS CVODE path the reference drives through FSPMat::action: CVodeCreate(
+ * CV_BDF, CV_NEWTON) with the matrix-free SPBCGS solver, RHS f(t,u) = A(t) u and J v = A(t) v
+ * (tests/test_sundials.cu:67-91, 142-200; problems/hog1p_5species.cu:203-228, 287-336).
+ * Variable order 1..5, quasi-constant step in backward-difference form, one GMRES solve of
+ * (I - c A(t_new)) d = rhs per step (the CME is linear), error weights
+ * 1 / (atol + rtol |p_i|) in the RMS norm (CVODE's), output times hit exactly (CVODE's tstop).
+ * All vectors stay on the device; the step control runs on the host, synchronous per step.
+ *
+ *   create:  coefs (host, n_reactions doubles) freezes c_r; NULL evaluates A's tcoef(t) at
+ *            every generator application (time-varying rates).  maxl: GMRES dimension, 1..60.
+ *   init:    t0 and the initial distribution (copied; the caller keeps d_p0).
+ *   advance: integrate to t_out and write p(t_out) to d_p.  one_step != 0 returns after one
+ *            internal step toward t_out (CV_ONE_STEP) with the time reached in *t_reached.
+ *   Errors: STEP_LIMIT when max_steps accepted steps do not reach t_out or the step size
+ *   underflows; NONFINITE when the solution or a coefficient stops being finite. */
+typedef struct cufsp_bdf_s cufsp_bdf;
+typedef struct {
+    double t;           /* time reached */
+    double h;           /* next step size */
+    double last_err;    /* weighted local error estimate of the last accepted step */
+    int order;          /* current BDF order */
+    int pad;
+    int64_t n_steps;    /* accepted steps since init */
+    int64_t n_reject;   /* steps rejected by the local error test */
+    int64_t n_matvec;   /* generator applications */
+    int64_t n_lin_iters;/* GMRES iterations */
+    int64_t n_lin_fail; /* GMRES solves that did not converge (step halved) */
+} cufsp_bdf_stats;
+cufsp_status cufsp_bdf_create(cufsp_mat *A, const double *coefs, double rtol, double atol, int maxl,
+                              cufsp_bdf **out);
+cufsp_status cufsp_bdf_destroy(cufsp_bdf *B);
+/* eps_lin: GMRES residual target in the weighted RMS norm (default 0.005); h_init <= 0: automatic
+ * starting step; h_max <= 0: unbounded; max_steps: accepted steps per init (default 10^6). */
+cufsp_status cufsp_bdf_set_options(cufsp_bdf *B, double eps_lin, double h_init, double h_max, int64_t max_steps);
+/* Replace the frozen coefficients (NULL: use A's tcoef(t)); takes effect at the next init. */
+cufsp_status cufsp_bdf_set_coefs(cufsp_bdf *B, const double *coefs);
+cufsp_status cufsp_bdf_init(cufsp_bdf *B, double t0, const double *d_p0, cufsp_stream_t stream);
+cufsp_status cufsp_bdf_advance(cufsp_bdf *B, double t_out, double *d_p, int one_step, cufsp_stream_t stream,
+                               double *t_reached);
+cufsp_status cufsp_bdf_get_stats(const cufsp_bdf *B, cufsp_bdf_stats *stats);
+
 /* ---- FSP solver through output times ------------------------------------------------------
  * Replaces cme::FSPSolver (src/FSPSolver.h:16-111, src/FSPSolver.cpp:9-22; never compiled in the
  * reference, semantics defined here): next_time() advances the caller's device vector p from the
@@ -182,6 +224,11 @@ typedef struct cufsp_solver_s cufsp_solver;
 cufsp_status cufsp_solver_create(cufsp_mat *A, const double *times, int n_times, double fsp_tol,
                                  const double *coefs, double kry_tol, int m, int iop, int q_iop,
                                  cufsp_solver **out);
+/* The same solver integrating with the BDF method (cufsp_bdf_*): coefs NULL follows A's tcoef(t)
+ * (time-varying rates).  The caller's vector is read at the first advance after create,
+ * reset_time or set_coefs (set_coefs(NULL) returns to tcoef(t)); krylov_steps then counts BDF steps. */
+cufsp_status cufsp_solver_create_bdf(cufsp_mat *A, const double *times, int n_times, double fsp_tol,
+                                     const double *coefs, double rtol, double atol, cufsp_solver **out);
 cufsp_status cufsp_solver_destroy(cufsp_solver *S);
 cufsp_status cufsp_solver_set_coefs(cufsp_solver *S, const double *coefs);
 cufsp_status cufsp_solver_next_time(cufsp_solver *S, double *d_p, cufsp_stream_t stream, cufsp_solver_status *status);

@@ -36,6 +36,17 @@ class ExpvStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class BdfStats(C.Structure):
+    _fields_ = [("t", C.c_double), ("h", C.c_double), ("last_err", C.c_double), ("order", C.c_int),
+                ("pad", C.c_int), ("n_steps", C.c_int64), ("n_reject", C.c_int64), ("n_matvec", C.c_int64),
+                ("n_lin_iters", C.c_int64), ("n_lin_fail", C.c_int64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}
+
+
+TCOEF_FN = C.CFUNCTYPE(None, C.c_double, C.POINTER(C.c_double), C.c_void_p)
+
 _lib = None
 _ref = None
 
@@ -72,6 +83,10 @@ def lib() -> C.CDLL:
         L.orc_expv.restype = _I
         L.orc_expv.argtypes = [_I64, _I, _P, _P, _P, _P, _D, _P, _I, _D, _I, _I, _D, _I64, _I64, C.POINTER(ExpvStats)]
         L.orc_num_threads.restype = _I
+        L.orc_bdf.restype = _I
+        L.orc_bdf.argtypes = [_I64, _I, _P, _P, _P, _P, TCOEF_FN, _P, _D, _P, _P, _I, _P, _D, _D, _I, _D, _D, _D,
+                              _I64, C.POINTER(BdfStats)]
+        L.orc_bdf_change_matrix.argtypes = [_I, _D, _P]
         _lib = L
     return _lib
 
@@ -234,6 +249,36 @@ def expv(csr: CSR, coefs, t_final: float, v, m: int = 30, tol: float = 1e-8, iop
                         float(tol), int(bool(iop)), int(q_iop), float(anorm), int(max_nstep), int(max_reject),
                         C.byref(st))
     return w, st.as_dict(), int(rc)
+
+
+def bdf(csr: CSR, coefs, t0: float, y0, times, rtol: float = 1e-8, atol: float = 1e-12, maxl: int = 30,
+        eps_lin: float = 0.005, h_init: float = 0.0, h_max: float = 0.0, max_steps: int = 10**6):
+    """Variable-order BDF for dp/dt = A(t) p (bdf_oracle.c, the CVODE path of tests/test_sundials.cu:67-200).
+    `coefs` is a coefficient array (time-invariant) or a callable t -> c(t).  Returns (Y [n_times, n], stats, rc)."""
+    times = _a(np.atleast_1d(times), np.float64)
+    y = _a(y0, np.float64)
+    out = np.empty((len(times), csr.n), np.float64)
+    if callable(coefs):
+        nr = csr.nr
+
+        def _tc(t, c, _user):
+            v = np.asarray(coefs(t), np.float64)
+            for r in range(nr):
+                c[r] = float(v[r])
+        cb, cp = TCOEF_FN(_tc), None
+    else:
+        cb, cp = TCOEF_FN(), _a(coefs, np.float64)
+    st = BdfStats()
+    rc = lib().orc_bdf(csr.n, csr.nr, _p(csr.rowptr), _p(csr.col), _p(csr.val), None if cp is None else _p(cp), cb,
+                       None, float(t0), _p(y), _p(times), len(times), _p(out), float(rtol), float(atol), int(maxl),
+                       float(eps_lin), float(h_init), float(h_max), int(max_steps), C.byref(st))
+    return out, st.as_dict(), int(rc)
+
+
+def bdf_change_matrix(k: int, rho: float) -> np.ndarray:
+    T = np.empty((k + 1, k + 1), np.float64)
+    lib().orc_bdf_change_matrix(int(k), float(rho), _p(T))
+    return T
 
 
 def toggle_factor_tables(bounds) -> np.ndarray:

@@ -127,3 +127,52 @@ def test_oracle_step_limit_and_zero_vector():
     assert oracle.ORC_ERR[rc] == "STEP_LIMIT"
     w, st, rc = oracle.expv(A, m.coefs(0), 10.0, np.zeros(m.n_states))
     assert rc == 0 and not w.any()
+
+
+def test_oracle_bdf_change_matrix_properties():
+    """Step-change matrix of the backward-difference BDF: identity at rho = 1 and a group in rho
+    (changing by a then by b equals changing by a*b)."""
+    for k in range(1, 6):
+        assert np.abs(oracle.bdf_change_matrix(k, 1.0) - np.eye(k + 1)).max() <= 1e-12
+        Ta, Tb, Tab = (oracle.bdf_change_matrix(k, r) for r in (0.5, 1.7, 0.85))
+        assert np.abs(Tb @ Ta - Tab).max() <= 1e-12 * max(1.0, np.abs(Tab).max())
+
+
+def test_oracle_bdf_matches_krylov_time_invariant():
+    m = models.birth_death_2()
+    A = oracle.assemble_model(m)
+    Y, st, rc = oracle.bdf(A, m.coefs(0), 0.0, m.p0(), [1.0, 10.0], rtol=1e-8, atol=1e-14)
+    assert rc == 0 and st["t"] == 10.0 and st["order"] >= 3
+    for t, y in zip((1.0, 10.0), Y):
+        ref, _, rc = oracle.expv(A, m.coefs(0), t, m.p0(), tol=1e-13)
+        assert np.abs(y - ref).sum() <= 1e-7
+
+
+def test_oracle_bdf_matches_scipy_time_varying():
+    """The reference's CVODE case (tests/test_sundials.cu:55-64: toggle switch with c_r(t)) on a
+    32^2 box, against SciPy's Radau at rtol 1e-12."""
+    import scipy.integrate as si
+    m = models.toggle((31, 31), time_varying=True)
+    A = oracle.assemble_model(m)
+    times = [50.0, 500.0]
+    Y, st, rc = oracle.bdf(A, m.coefs, 0.0, m.p0(), times, rtol=1e-9, atol=1e-14)
+    assert rc == 0 and st["n_lin_fail"] == 0
+    Ms = [A.to_scipy(np.eye(A.nr)[r]) for r in range(A.nr)]
+
+    def jac(t, y):
+        c = m.coefs(t)
+        return sum(c[r] * Ms[r] for r in range(A.nr))
+    sol = si.solve_ivp(lambda t, y: jac(t, y) @ y, (0.0, times[-1]), m.p0(), method="Radau", t_eval=times,
+                       rtol=1e-12, atol=1e-16, jac=jac)
+    assert sol.status == 0
+    for k in range(len(times)):
+        assert np.abs(Y[k] - sol.y[:, k]).sum() <= 1e-7
+
+
+def test_oracle_bdf_limits():
+    m = models.birth_death_2()
+    A = oracle.assemble_model(m)
+    _, _, rc = oracle.bdf(A, m.coefs(0), 0.0, m.p0(), [10.0], max_steps=3)
+    assert oracle.ORC_ERR[rc] == "STEP_LIMIT"
+    Y, st, rc = oracle.bdf(A, m.coefs(0), 0.0, m.p0(), [0.0, 0.0])
+    assert rc == 0 and st["n_steps"] == 0 and np.array_equal(Y[1], m.p0())
