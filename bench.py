@@ -260,7 +260,8 @@ def run_ours(args):
     if args.no_extras:  # profiling runs: the timed generator action only
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": round(value, 3), "unit": "GB/s", "ms_per_step": round(ms, 5),
-                              "steps": args.steps, "sets": n_sets, "profiling_run": True}), flush=True)
+                              "steps": args.steps, "sets": n_sets, "profiling_run": True, "kernel": A.describe()}),
+                  flush=True)
         if world > 1:
             dist.destroy_process_group()
         return
@@ -301,7 +302,7 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "achieved": round(kernel_gbs, 3), "peak": peak, "unit": "GB/s",
                          "frac": round(kernel_gbs / peak, 4), "traffic": profile_traffic(),
                          "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured" else "fallback 6.65 TB/s",
-                         "kernel": "k_kron_mv (cufsp_kron.cu)"},
+                         "kernel": A.describe()},
             "cpu_baseline": ({k: (round(v, 3) if isinstance(v, float) else v) for k, v in cpu.items() if k != "ms_per_step"}
                              if cpu else None),
             "clocks": clk,

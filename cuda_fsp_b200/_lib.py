@@ -94,6 +94,7 @@ SIGNATURES = {
     "cufsp_mat_action_host": [_P, C.c_double, _P, _P],
     "cufsp_mat_export_propensities": [_P, _P, _P],
     "cufsp_mat_watchdog": [_P, _IP],
+    "cufsp_mat_describe": [_P, C.c_char_p, C.c_size_t],
     "cufsp_expv_create": [C.c_int64, C.c_int, C.c_double, C.c_int, C.c_int, C.c_double, C.POINTER(_P)],
     "cufsp_expv_destroy": [_P],
     "cufsp_expv_set_limits": [_P, C.c_int64, C.c_int64],

@@ -26,10 +26,13 @@ OBJ = PKG / "_build"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-rdc=true", "-Xcompiler", "-fPIC,-O2",
                      "-I" + str(ROOT / "include"), "--expt-relaxed-constexpr", "--extended-lambda"]
-SOURCES = ["cufsp_common.cu", "cufsp_kron.cu", "cufsp_kron_march.cu", "cufsp_sparse.cu", "cufsp_mat.cu",
+SOURCES = ["cufsp_common.cu", "cufsp_kron.cu", "cufsp_kron_plane.cu", "cufsp_kron_march.cu", "cufsp_sparse.cu", "cufsp_mat.cu",
            "cufsp_krylov.cu", "cufsp_expm.cpp", "cufsp_noalloc.cu", "cufsp_stats.cu", "cufsp_solver.cu",
            "cufsp_vec.cu", "cufsp_bdf.cu"]
-HEADERS = ["cufsp_internal.h", "cufsp_reduce.cuh", "cufsp_march.h", "cufsp_vec.h"]
+HEADERS = ["cufsp_internal.h", "cufsp_reduce.cuh", "cufsp_march.h", "cufsp_vec.h", "cufsp_plane.cuh"]
+# Kernel sources compiled at run time by NVRTC are embedded in the library as string literals.
+RTC_SOURCES = {"cufsp_plane.cuh": "cufsp_plane_src.inc"}
+LINK_LIBS = ["-L/usr/local/cuda/lib64", "-lnvrtc", "-Xlinker", "-rpath,/usr/local/cuda/lib64"]
 
 
 def nvcc() -> str:
@@ -53,17 +56,31 @@ def _run(cmd: list[str]) -> None:
         raise RuntimeError(f"build step failed: {cmd[-1]}")
 
 
+def _embed_rtc_sources(force: bool) -> None:
+    """Write each NVRTC kernel source as a raw string literal into the build folder."""
+    for src, inc in RTC_SOURCES.items():
+        text = (CSRC / src).read_text()
+        if ")CUFSPSRC" in text:
+            raise RuntimeError(f"{src} contains the raw-string delimiter")
+        out = OBJ / inc
+        body = 'R"CUFSPSRC(' + text + ')CUFSPSRC"\n'
+        if force or not out.exists() or out.read_text() != body:
+            out.write_text(body)
+
+
 def _compile(src: Path, obj: Path, extra: list[str], force: bool) -> Path:
     deps = [src] + [CSRC / h for h in HEADERS] + [ROOT / "include" / "cufsp.h"]
+    deps += [OBJ / inc for inc in RTC_SOURCES.values()]
     if force or _stale(obj, deps):
         obj.parent.mkdir(parents=True, exist_ok=True)
-        _run([nvcc()] + NVCC_FLAGS + extra + ["-c", str(src), "-o", str(obj)])
+        _run([nvcc()] + NVCC_FLAGS + ["-I" + str(OBJ)] + extra + ["-c", str(src), "-o", str(obj)])
     return obj
 
 
 def build(force: bool = False, verbose: bool = False) -> dict[str, Path]:
     LIB.mkdir(parents=True, exist_ok=True)
     OBJ.mkdir(parents=True, exist_ok=True)
+    _embed_rtc_sources(force)
     srcs = [CSRC / s for s in SOURCES]
     support = ROOT / "tests" / "support" / "test_models.cu"
     cpp_test = ROOT / "tests" / "cpp" / "test_dropin.cu"
@@ -78,7 +95,7 @@ def build(force: bool = False, verbose: bool = False) -> dict[str, Path]:
     out = {}
     so = LIB / "libcufsp.so"
     if force or _stale(so, [Path(o) for o in lib_objs]):
-        _run([nvcc()] + ARCH + ["-shared", "-rdc=true", "-Xcompiler", "-fPIC"] + lib_objs + ["-o", str(so)])
+        _run([nvcc()] + ARCH + ["-shared", "-rdc=true", "-Xcompiler", "-fPIC"] + lib_objs + LINK_LIBS + ["-o", str(so)])
     out["libcufsp"] = so
     ar = LIB / "libcufsp_static.a"
     if force or _stale(ar, [Path(o) for o in lib_objs]):
@@ -88,13 +105,14 @@ def build(force: bool = False, verbose: bool = False) -> dict[str, Path]:
         tso = ROOT / "tests" / "support" / "libcufsp_testmodels.so"
         tobj = str(OBJ / "test_models.cu.o")
         if force or _stale(tso, [Path(o) for o in lib_objs] + [Path(tobj)]):
-            _run([nvcc()] + ARCH + ["-shared", "-rdc=true", "-Xcompiler", "-fPIC"] + lib_objs + [tobj, "-o", str(tso)])
+            _run([nvcc()] + ARCH + ["-shared", "-rdc=true", "-Xcompiler", "-fPIC"] + lib_objs + [tobj] + LINK_LIBS
+                 + ["-o", str(tso)])
         out["testmodels"] = tso
     if cpp_test.exists():
         exe = ROOT / "tests" / "cpp" / "test_dropin"
         cobj = str(OBJ / "test_dropin.cu.o")
         if force or _stale(exe, [Path(o) for o in lib_objs] + [Path(cobj)]):
-            _run([nvcc()] + ARCH + ["-rdc=true", cobj, str(ar), "-o", str(exe)])
+            _run([nvcc()] + ARCH + ["-rdc=true", cobj, str(ar)] + LINK_LIBS + ["-o", str(exe)])
         out["test_dropin"] = exe
     if verbose:
         for k, v in out.items():

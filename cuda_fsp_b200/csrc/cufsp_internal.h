@@ -116,6 +116,23 @@ cufsp_status sparse_apply(SparseData *s, const double *coefs, double alpha, cons
 cufsp_status sparse_export(const SparseData *s, double *d_props, cudaStream_t st);
 int64_t sparse_halo(const SparseData *s);
 
+// Runtime-specialised plane kernel for near-neighbour networks of 2-3 species (cufsp_kron_plane.cu).
+struct PlaneData;
+// nullptr (with the reason in `why`) when the network does not have the plane kernel's shape or the
+// kernel could not be compiled; d_tables: the generator's device factor tables.
+PlaneData *plane_create(const ModelHost &m, const double *d_tables, std::string &why);
+void plane_destroy(PlaneData *pd);
+const std::string &plane_description(const PlaneData *pd);
+int64_t plane_size(const PlaneData *pd);  // states per plane (slab granularity)
+int plane_watchdog(PlaneData *pd);         // 1 if a bounded barrier wait expired since the last call (reset)
+// false when this apply is not for the plane kernel (range not whole planes, unaligned vectors);
+// otherwise launches and sets *status.
+bool plane_launch(PlaneData *pd, const double *coefs, double alpha, const double *d_alpha, const int *d_skip,
+                  const double *x, bool accumulate, double *y, cudaStream_t st, int64_t i_begin, int64_t i_end,
+                  cufsp_status *status);
+// Human-readable kernel choice of a KRONECKER generator.
+std::string kron_describe(const KronData *k);
+
 // Host-side dense exponential (cufsp_expm.cpp).
 cufsp_status expm_pade13(int k, const double *A, double *F);
 

@@ -308,6 +308,9 @@ struct KronData {
     size_t march_smem = 0;
     int *d_err = nullptr;
     double2 *d_gtab_march = nullptr;  // only when the marching split differs from k
+    // runtime-specialised plane kernel (cufsp_kron_plane.cu), when the network has its shape
+    PlaneData *plane = nullptr;
+    std::string plane_why;
 };
 
 // Outer factor table for the inner split k: G[q][r] = (prod_{s>=k} f_{r,s}(x_s - nu_{r,s}), or 0
@@ -628,6 +631,7 @@ cufsp_status kron_create(const ModelHost &m, KronData **out) {
         kron_destroy(kd);
         return cuda_error(e, "kron_create");
     }
+    kd->plane = plane_create(m, kd->d_tables, kd->plane_why);
     plan_march(m, kd);
     if (kd->march && kd->ma.k != kd->k) {  // the marching split needs its own outer table
         const std::vector<double2> gm = outer_table(m, kd, kd->ma.k);
@@ -648,22 +652,37 @@ void kron_destroy(KronData *k) {
     if (k->d_gtab) cudaFree(k->d_gtab);
     if (k->d_gtab_march) cudaFree(k->d_gtab_march);
     if (k->d_err) cudaFree(k->d_err);
+    plane_destroy(k->plane);
     delete k;
 }
 
 int kron_watchdog(KronData *k) {
-    if (!k || !k->d_err) return 0;
+    if (!k) return 0;
+    int pv = k->plane ? plane_watchdog(k->plane) : 0;
+    if (pv < 0) return -1;
+    if (!k->d_err) return pv;
     int v = 0;
     if (cudaMemcpy(&v, k->d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
     if (v) cudaMemset(k->d_err, 0, sizeof(int));
-    return v;
+    return v | pv;
 }
 
-int64_t kron_halo(const KronData *k) { return k->halo; }
-int64_t kron_row_len(const KronData *k) { return k->L; }
+// The plane kernel reads one plane beyond each end of the range it computes.
+int64_t kron_halo(const KronData *k) { return k->plane ? std::max<int64_t>(k->halo, plane_size(k->plane)) : k->halo; }
+int64_t kron_row_len(const KronData *k) { return k->plane ? plane_size(k->plane) : k->L; }
+
+std::string kron_describe(const KronData *k) {
+    if (k->plane) return plane_description(k->plane);
+    return "k_kron_mv (NR=" + std::to_string(k->NR) + " NG=" + std::to_string(k->NG) + " V=" + std::to_string(k->V) +
+           " inner species=" + std::to_string(k->k) + "); plane kernel not used: " + k->plane_why;
+}
 
 cufsp_status kron_apply(KronData *kd, const double *coefs, double alpha, const double *d_alpha, const int *d_skip,
                         const double *x, bool accumulate, double *y, cudaStream_t st, int64_t i_begin, int64_t i_end) {
+    if (kd->plane) {
+        cufsp_status ps = CUFSP_SUCCESS;
+        if (plane_launch(kd->plane, coefs, alpha, d_alpha, d_skip, x, accumulate, y, st, i_begin, i_end, &ps)) return ps;
+    }
     const bool full = i_begin == 0 && (i_end < 0 || i_end == kd->n);
     if (kd->march && full && (reinterpret_cast<uintptr_t>(x) % 16) == 0) {
         MarchArgs ma = kd->ma;

@@ -2,6 +2,7 @@
 // src/FSPMat.h:21-56, src/FSPMat.cu:10-118).
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 
 #include "cufsp_internal.h"
 
@@ -104,6 +105,15 @@ extern "C" cufsp_status cufsp_mat_watchdog(cufsp_mat *A, int *tripped) {
     const int v = A->kron ? kron_watchdog(A->kron) : 0;
     if (v < 0) return set_error(CUFSP_ERR_CUDA, "cufsp_mat_watchdog: device read failed");
     *tripped = v;
+    return CUFSP_SUCCESS;
+}
+
+extern "C" cufsp_status cufsp_mat_describe(const cufsp_mat *A, char *buf, size_t len) {
+    if (!A || !buf || len == 0) return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_mat_describe: bad argument");
+    const std::string d = A->kron ? "KRONECKER: " + kron_describe(A->kron) : std::string("sparse: k_sparse_mv");
+    const size_t k = std::min(len - 1, d.size());
+    std::memcpy(buf, d.data(), k);
+    buf[k] = 0;
     return CUFSP_SUCCESS;
 }
 

@@ -175,6 +175,13 @@ class FSPMat:
         _lib.check(self._lib, self._lib.cufsp_mat_watchdog(self._h, C.byref(t)), "cufsp_mat_watchdog")
         return int(t.value)
 
+    def describe(self) -> str:
+        """The kernel that serves this generator's action (and, for KRONECKER generators that do
+        not use the runtime-specialised plane kernel, why not)."""
+        buf = C.create_string_buffer(1024)
+        _lib.check(self._lib, self._lib.cufsp_mat_describe(self._h, buf, len(buf)), "cufsp_mat_describe")
+        return buf.value.decode()
+
     def export_propensities(self):
         import torch
         out = torch.empty((self.nr, self.n), dtype=torch.float64, device="cuda")

@@ -121,6 +121,11 @@ cufsp_status cufsp_mat_action_host(cufsp_mat *A, double t, const double *x_host,
  * is reset.  Synchronises the device. */
 cufsp_status cufsp_mat_watchdog(cufsp_mat *A, int *tripped);
 
+/* Which kernel serves this generator's action, as text (e.g. the runtime-specialised plane kernel of
+ * a KRONECKER generator, or the general one with the reason the plane kernel was not used).
+ * Writes at most len bytes including the terminating NUL.  No counterpart in the reference. */
+cufsp_status cufsp_mat_describe(const cufsp_mat *A, char *buf, size_t len);
+
 /* Sparse-format export for checking (HYB/CSR formats only): props[r*n + i] = a_r(x_i). */
 cufsp_status cufsp_mat_export_propensities(const cufsp_mat *A, double *d_props, cufsp_stream_t stream);
 
