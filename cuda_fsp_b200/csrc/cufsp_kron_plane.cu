@@ -247,38 +247,45 @@ PlaneData *plane_create(const ModelHost &m, const double *d_tables, std::string 
         pd->wa.r_dg[r] = r_dg[r];
     }
     // tile rows (dividing n1) and ring stages
-    int tr = 1;
-    if (rows) {
-        const int want = env_int("CUFSP_PLANE_TR", 4);
-        for (int cand : {want, 4, 2, 1})
-            if (cand >= 1 && cand <= 8 && pd->n1 % cand == 0) {
-                tr = cand;
-                break;
-            }
-    }
-    pd->tr = tr;
-    const int nq = rows ? tr + 2 : 1;
+    // Tile rows TR (dividing n1) and ring stages S: the preferred pair (TR = 2, S = 5 unless set by
+    // CUFSP_PLANE_TR / CUFSP_PLANE_STAGES), stepping down -- fewer stages first, then lower tiles --
+    // until the ring fits the shared memory of one SM.
     const int chunks = (n0 + 63) / 64;
     pd->threads = 32 * chunks;
     pd->pitch = 64 * chunks;
-    pd->row_blocks = pd->n1 / tr;
-    const int stages = std::max(3, std::min(12, env_int("CUFSP_PLANE_STAGES", 5)));
     const int ytma = env_int("CUFSP_PLANE_YTMA", 1) != 0 ? 1 : 0;
-    auto stage_bytes = [&](bool accum) {
-        return (size_t)8 * ((size_t)(nq + (accum && ytma ? tr : 0)) * pd->pitch + (size_t)tr * pd->wa.nwp);
-    };
-    pd->smem_accum = stages * stage_bytes(true);
-    pd->smem_set = stages * stage_bytes(false);
     const DeviceInfo &di = device_info();
+    const int want_tr = env_int("CUFSP_PLANE_TR", 2);
+    const int want_s = std::max(3, std::min(12, env_int("CUFSP_PLANE_STAGES", 5)));
+    auto stage_bytes = [&](int tr_, bool accum) {
+        const int nq_ = rows ? tr_ + 2 : 1;
+        return (size_t)8 * ((size_t)(nq_ + (accum && ytma ? tr_ : 0)) * pd->pitch + (size_t)tr_ * pd->wa.nwp);
+    };
+    int tr = 0, stages = 0;
+    for (int cand : {want_tr, 4, 2, 1}) {
+        if (tr) break;
+        if (cand < 1 || cand > 8 || (rows ? pd->n1 % cand != 0 : cand != 1)) continue;
+        if (cand > want_tr && want_tr >= 1) continue;
+        for (int st = want_s; st >= 3; --st)
+            if (st * stage_bytes(cand, true) <= (size_t)di.max_smem_optin) {
+                tr = cand;
+                stages = st;
+                break;
+            }
+    }
+    if (!tr) {
+        why = "ring stages exceed shared memory";
+        return nullptr;
+    }
+    pd->tr = tr;
+    pd->row_blocks = pd->n1 / tr;
+    pd->smem_accum = stages * stage_bytes(tr, true);
+    pd->smem_set = stages * stage_bytes(tr, false);
     // CTAs per SM the launch bounds promise: as many as the ring stages fit in shared memory, but
     // never so many that a thread gets fewer than 128 registers.
     const int by_smem = (int)std::max<size_t>(1, (size_t)(di.max_smem_optin + 1024) / (pd->smem_accum + 1024));
     const int by_regs = std::max(1, 65536 / (128 * pd->threads));
     const int minb = std::max(1, std::min(16, env_int("CUFSP_PLANE_MINB", std::min(by_smem, by_regs))));
-    if (pd->smem_accum > (size_t)di.max_smem_optin) {
-        why = "ring stages exceed shared memory";
-        return nullptr;
-    }
     std::ostringstream s;
     s << "#define CUFSP_PLANE_NR " << nr << "\n#define CUFSP_PLANE_NOFF " << offs.size() << "\n#define CUFSP_PLANE_NFA "
       << fa_tabs.size() << "\n#define CUFSP_PLANE_NFB " << fb_tabs.size() << "\n#define CUFSP_PLANE_NT " << terms.size()
