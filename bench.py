@@ -55,7 +55,7 @@ def measured_peak_hbm() -> tuple[float, str]:
 
 def profile_traffic() -> float | None:
     """DRAM bytes per launch of the KRONECKER action from the committed ncu summary, if present."""
-    p = ROOT / "profiles" / "kron_mv_mass_action_3.md"
+    p = ROOT / "profiles" / "kron_plane_mass_action_3.md"
     if not p.exists():
         return None
     for line in p.read_text().splitlines():

@@ -257,6 +257,53 @@ cufsp_status cufsp_ssa(const cufsp_model_desc *desc, const double *coefs, const 
                        int n_times, int n_cells, unsigned long long seed, int64_t max_events, int *d_out,
                        cufsp_stream_t stream);
 
+/* ---- batched exp(tA)p over many instances, one persistent launch ---------------------------
+ * No counterpart in the reference, which solves one instance per KryExpvFSP object; this is the
+ * batched form of KryExpvFSP::solve (src/KryExpvFSP.cu:184-188) for parameter sweeps and
+ * likelihood evaluations.  Instances share one reaction network (stoichiometry) but each has its
+ * own box, factor tables and rate coefficients.  The whole adaptive Krylov solve -- Arnoldi, the
+ * Pade exponential of the small Hessenberg matrix and the Expokit step control -- runs on the
+ * device, one thread-block cluster per instance at a time, replayed as a CUDA graph.
+ *   create:  fsp_bounds [n_instances][n_species]; factor_tables[i] -> n_reactions * sum_s (b_s + 1)
+ *            doubles in the reference layout (as cufsp_model_desc); coefs [n_instances][n_reactions].
+ *            m <= 32; iop / q_iop: incomplete orthogonalisation as in cufsp_expv_create.
+ *   layout:  offsets (host, n_instances + 1): instance i's vector occupies
+ *            [offsets[i], offsets[i] + n_i) of the packed device array; offsets[n] = total length.
+ *   solve:   d_packed in: p(0) of every instance, out: exp(t_final A_i) p_i(0).  The first solve
+ *            chooses the launch shape (autotuner, cached per device and network) unless
+ *            cufsp_batch_set_shape fixed it.  Synchronous; stats (host, n_instances, or NULL).
+ *            Returns STEP_LIMIT / NONFINITE if any instance failed (see its stat.status). */
+typedef struct {
+    int n_species;
+    int n_reactions;
+    const int *stoich_vals;
+    const int *stoich_colidxs;
+    const int *stoich_rowptrs;
+    int n_instances;
+    const int *fsp_bounds;
+    const double *const *factor_tables;
+    const double *coefs;
+} cufsp_batch_desc;
+typedef struct {
+    double t;        /* time reached */
+    double err;      /* last local error estimate */
+    int steps;       /* accepted Krylov steps */
+    int rejects;     /* rejected step sizes */
+    int matvecs;     /* generator applications */
+    int status;      /* 0 ok, 1 step limit, 2 NaN/Inf */
+} cufsp_batch_stat;
+typedef struct cufsp_batch_s cufsp_batch;
+cufsp_status cufsp_batch_create(const cufsp_batch_desc *desc, int m, double tol, int iop, int q_iop, cufsp_batch **out);
+cufsp_status cufsp_batch_destroy(cufsp_batch *B);
+cufsp_status cufsp_batch_layout(const cufsp_batch *B, int64_t *offsets);
+cufsp_status cufsp_batch_set_coefs(cufsp_batch *B, const double *coefs);
+cufsp_status cufsp_batch_set_limits(cufsp_batch *B, int max_steps, int max_reject);
+/* Fix the launch shape (CTAs per cluster 1..16, threads 128/256/512); (0, 0) re-enables the autotuner. */
+cufsp_status cufsp_batch_set_shape(cufsp_batch *B, int cluster_ctas, int threads);
+cufsp_status cufsp_batch_solve(cufsp_batch *B, double t_final, double *d_packed, cufsp_stream_t stream,
+                               cufsp_batch_stat *stats);
+cufsp_status cufsp_batch_describe(const cufsp_batch *B, char *buf, size_t len);
+
 /* Dense exponential of a k x k column-major host matrix by scaling-and-squaring Pade(13,13)
  * (replaces arma::expmat at src/KryExpvFSP.cu:125). */
 cufsp_status cufsp_expm_host(int k, const double *A, double *F);
