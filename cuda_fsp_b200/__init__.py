@@ -6,9 +6,10 @@ the BDF integrator that replaces its CVODE path) plus the workload definitions i
 """
 from . import models
 from ._lib import CufspError
+from .batch import BatchKrylov
 from .fsp import FSPMat, KryExpvFSP, MatrixFormat, expm, get_states, num_states
 from .likelihood import FSPSolver, Likelihood, generate_data, histograms
 from .ode import BDFIntegrator
 
-__all__ = ["models", "CufspError", "FSPMat", "KryExpvFSP", "MatrixFormat", "expm", "get_states", "num_states",
+__all__ = ["models", "CufspError", "BatchKrylov", "FSPMat", "KryExpvFSP", "MatrixFormat", "expm", "get_states", "num_states",
            "FSPSolver", "Likelihood", "generate_data", "histograms", "BDFIntegrator"]

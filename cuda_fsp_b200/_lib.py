@@ -72,6 +72,28 @@ class BdfStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "pad"}
 
 
+class BatchDesc(C.Structure):
+    _fields_ = [
+        ("n_species", C.c_int),
+        ("n_reactions", C.c_int),
+        ("stoich_vals", C.POINTER(C.c_int)),
+        ("stoich_colidxs", C.POINTER(C.c_int)),
+        ("stoich_rowptrs", C.POINTER(C.c_int)),
+        ("n_instances", C.c_int),
+        ("fsp_bounds", C.POINTER(C.c_int)),
+        ("factor_tables", C.POINTER(C.POINTER(C.c_double))),
+        ("coefs", C.POINTER(C.c_double)),
+    ]
+
+
+class BatchStat(C.Structure):
+    _fields_ = [("t", C.c_double), ("err", C.c_double), ("steps", C.c_int), ("rejects", C.c_int),
+                ("matvecs", C.c_int), ("status", C.c_int)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 _P = C.c_void_p
 _I64P = C.POINTER(C.c_int64)
 _IP = C.POINTER(C.c_int)
@@ -125,6 +147,14 @@ SIGNATURES = {
     "cufsp_loglik": [C.c_int64, _P, C.c_int64, _P, _DP, _P],
     "cufsp_ssa": [C.POINTER(ModelDesc), _DP, _IP, _DP, C.c_int, C.c_int, C.c_ulonglong, C.c_int64, _P, _P],
     "cufsp_vec_sum": [C.c_int64, _P, _DP, _P],
+    "cufsp_batch_create": [C.POINTER(BatchDesc), C.c_int, C.c_double, C.c_int, C.c_int, C.POINTER(_P)],
+    "cufsp_batch_destroy": [_P],
+    "cufsp_batch_layout": [_P, _I64P],
+    "cufsp_batch_set_coefs": [_P, _DP],
+    "cufsp_batch_set_limits": [_P, C.c_int, C.c_int],
+    "cufsp_batch_set_shape": [_P, C.c_int, C.c_int],
+    "cufsp_batch_solve": [_P, C.c_double, _P, _P, C.POINTER(BatchStat)],
+    "cufsp_batch_describe": [_P, C.c_char_p, C.c_size_t],
     "cufsp_vec_sum_noalloc": [C.c_int64, _P, _P, _P],
 }
 _RESTYPE = {"cufsp_status_string": C.c_char_p, "cufsp_last_error": C.c_char_p}

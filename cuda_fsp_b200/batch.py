@@ -1,0 +1,119 @@
+"""Batched exp(tA)p over many FSP instances in one persistent launch (cufsp_batch_* in cufsp.h).
+
+The reference solves one instance per KryExpvFSP object (src/KryExpvFSP.cu:184-188); parameter
+sweeps and likelihood evaluations there loop over objects.  BatchKrylov solves hundreds of instances
+of one reaction network -- each with its own box, factor tables and rates -- to a common final
+time with the whole adaptive Krylov solve on the device.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import BatchDesc, BatchStat
+from .fsp import _ptr, _stream
+
+
+class BatchKrylov:
+    """Instances share `nu` ([n_reactions, n_species] net changes); instance i has bounds[i],
+    factor tables tables[i] ([n_reactions, sum_s(b_s + 1)], the reference layout) and rate
+    coefficients coefs[i].  m <= 32, tol as KryExpvFSP; iop / q_iop: incomplete orthogonalisation."""
+
+    def __init__(self, nu, bounds, tables, coefs, m: int = 30, tol: float = 1e-8, iop: bool = False, q_iop: int = 2,
+                 lib: C.CDLL | None = None):
+        self._lib = lib or _lib.load()
+        nu = np.asarray(nu, np.int32)
+        self.nr, self.ns = nu.shape
+        self.n_instances = len(bounds)
+        vals, cols, rows = [], [], [0]
+        for r in range(self.nr):
+            for s in range(self.ns):
+                if nu[r, s]:
+                    vals.append(int(nu[r, s]))
+                    cols.append(s)
+            rows.append(len(vals))
+        self._vals = np.asarray(vals or [0], np.int32)
+        self._cols = np.asarray(cols or [0], np.int32)
+        self._rows = np.asarray(rows, np.int32)
+        self._bounds = np.ascontiguousarray(np.asarray(bounds, np.int32).reshape(self.n_instances, self.ns))
+        self._tabs = [np.ascontiguousarray(np.asarray(t, np.float64)) for t in tables]
+        self._coefs = np.ascontiguousarray(np.asarray(coefs, np.float64).reshape(self.n_instances, self.nr))
+        tab_ptrs = (C.POINTER(C.c_double) * self.n_instances)(
+            *[t.ctypes.data_as(C.POINTER(C.c_double)) for t in self._tabs])
+        ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int))  # noqa: E731
+        d = BatchDesc(self.ns, self.nr, ip(self._vals), ip(self._cols), ip(self._rows), self.n_instances,
+                      ip(self._bounds), tab_ptrs, self._coefs.ctypes.data_as(C.POINTER(C.c_double)))
+        h = C.c_void_p()
+        _lib.check(self._lib, self._lib.cufsp_batch_create(C.byref(d), int(m), float(tol), int(bool(iop)), int(q_iop),
+                                                           C.byref(h)), "cufsp_batch_create")
+        self._h = h
+        off = np.zeros(self.n_instances + 1, np.int64)
+        _lib.check(self._lib, self._lib.cufsp_batch_layout(self._h, off.ctypes.data_as(C.POINTER(C.c_int64))),
+                   "cufsp_batch_layout")
+        self.offsets = off
+        self.sizes = np.prod(self._bounds + 1, axis=1).astype(np.int64)
+
+    @classmethod
+    def from_models(cls, models_, m: int = 30, tol: float = 1e-8, iop: bool = False, q_iop: int = 2):
+        nu = models_[0].nu
+        for mm in models_:
+            if not np.array_equal(mm.nu, nu):
+                raise ValueError("all instances of a batch share one stoichiometry")
+        return cls(nu, [mm.bounds for mm in models_], [mm.tables for mm in models_],
+                   np.stack([mm.coefs(0.0) for mm in models_]), m=m, tol=tol, iop=iop, q_iop=q_iop)
+
+    @property
+    def total(self) -> int:
+        return int(self.offsets[-1])
+
+    def pack(self, vectors):
+        """Host vectors (one per instance) -> packed device tensor."""
+        import torch
+        buf = np.zeros(self.total)
+        for i, v in enumerate(vectors):
+            buf[self.offsets[i]:self.offsets[i] + self.sizes[i]] = v
+        return torch.as_tensor(buf, device="cuda")
+
+    def unpack(self, packed) -> list[np.ndarray]:
+        a = packed.detach().cpu().numpy() if hasattr(packed, "detach") else np.asarray(packed)
+        return [a[self.offsets[i]:self.offsets[i] + self.sizes[i]].copy() for i in range(self.n_instances)]
+
+    def set_coefs(self, coefs) -> None:
+        c = np.ascontiguousarray(np.asarray(coefs, np.float64).reshape(self.n_instances, self.nr))
+        _lib.check(self._lib, self._lib.cufsp_batch_set_coefs(self._h, c.ctypes.data_as(C.POINTER(C.c_double))),
+                   "cufsp_batch_set_coefs")
+
+    def set_limits(self, max_steps: int, max_reject: int) -> None:
+        _lib.check(self._lib, self._lib.cufsp_batch_set_limits(self._h, int(max_steps), int(max_reject)),
+                   "cufsp_batch_set_limits")
+
+    def set_shape(self, cluster_ctas: int = 0, threads: int = 0) -> None:
+        """Fix the launch shape; (0, 0) lets the autotuner choose at the next solve."""
+        _lib.check(self._lib, self._lib.cufsp_batch_set_shape(self._h, int(cluster_ctas), int(threads)),
+                   "cufsp_batch_set_shape")
+
+    def solve(self, t_final: float, packed, stream=None, check: bool = True) -> list[dict]:
+        """packed (device, float64, length total): p(0) in, exp(t_final A_i) p_i(0) out."""
+        st = (BatchStat * self.n_instances)()
+        rc = self._lib.cufsp_batch_solve(self._h, float(t_final), _ptr(packed), _stream(stream), st)
+        if check:
+            _lib.check(self._lib, rc, "cufsp_batch_solve")
+        return [s.as_dict() for s in st]
+
+    def describe(self) -> str:
+        buf = C.create_string_buffer(512)
+        _lib.check(self._lib, self._lib.cufsp_batch_describe(self._h, buf, len(buf)), "cufsp_batch_describe")
+        return buf.value.decode()
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.cufsp_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

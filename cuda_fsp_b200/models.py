@@ -13,6 +13,7 @@ Workloads (synthetic, seeded):
                    box 1x1x1x127x127 (131,072 states), one switching rate k0*sigmoid((t-5)/0.5)
   mass_action_3    3 species, 9 mass-action reactions, rates log-uniform in [1e-2, 10] from seed
                    20261203, box 255^3 (16,777,216 states), p0 = Poisson(5)^3
+  gene_batch       parameter sets of gene_expression with uneven boxes (batched solves)
 """
 from __future__ import annotations
 
@@ -206,3 +207,15 @@ def mass_action_3(bound=255, seed=20261203, bounds=None) -> CMEModel:
     orders = [[0, 0, 0], [0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1], [1, 0, 0], [0, 1, 0], [1, 1, 0], [1, 0, 1]]
     b = tuple(bounds) if bounds is not None else (bound, bound, bound)
     return mass_action(b, nu, orders, rates, name="mass_action_3", p0_kind="poisson5", meta={"seed": seed})
+
+
+def gene_batch(n: int = 256, seed: int = 20261204, lo: int = 63, hi: int = 255) -> list[CMEModel]:
+    """n parameter sets of gene_expression with time-invariant rates: every rate log-uniform within
+    one decade of its nominal value, nuclear and cytoplasmic mRNA bounds uniform in lo..hi."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        scale = 10.0 ** rng.uniform(-1.0, 1.0, size=12)
+        bn, bc = (int(v) for v in rng.integers(lo, hi + 1, size=2))
+        out.append(gene_expression((1, 1, 1, bn, bc), time_varying=False, rates_scale=scale))
+    return out
