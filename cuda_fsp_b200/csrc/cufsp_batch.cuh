@@ -109,19 +109,117 @@ struct Shared {
     int flag[4];
 };
 
-// Cluster-wide sum of K partial sums (acc[k] per thread): every CTA ends with the totals in s.tot.
-template <int K>
-__device__ __forceinline__ void cluster_sum(cg::cluster_group &cl, Shared &s, double (&acc)[K], int kused, int &buf) {
+// Cluster-wide sum of one value per thread: every CTA ends with the total in s.tot[0].
+__device__ __forceinline__ void cluster_sum1(cg::cluster_group &cl, Shared &s, double v, int &buf);
+
+// Constants of the current instance, copied into registers for the generator action.
+struct Regs {
+    double coef[NR];
+    int delta[NR];
+    int dims[NS];
+    CufspBatchDiv div[NS];
+    int tab_off[NS];
+    int tab_stride;
+};
+
+__device__ __forceinline__ void load_regs(const CufspBatchInst &in, Regs &g) {
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+        g.coef[r] = in.coef[r];
+        g.delta[r] = in.delta[r];
+    }
+#pragma unroll
+    for (int sp = 0; sp < NS; ++sp) {
+        g.dims[sp] = in.dims[sp];
+        g.div[sp] = in.div[sp];
+        g.tab_off[sp] = in.tab_off[sp];
+    }
+    g.tab_stride = in.tab_stride;
+}
+
+// Factor f_{r,s}(x) of the current instance.
+template <int R, int SP>
+__device__ __forceinline__ double factor(const Regs &g, const double *__restrict__ tab, int x) {
+    if constexpr (kind(R, SP) == 0) return 1.0;
+    else if constexpr (kind(R, SP) == 1) return (double)x;
+    else return __ldg(tab + R * g.tab_stride + g.tab_off[SP] + x);
+}
+
+template <int R, int SP>
+__device__ __forceinline__ void src_factor(const Regs &g, const double *__restrict__ tab, const int (&x)[NS], double &f,
+                                           bool &ok) {
+    if constexpr (SP < NS) {
+        const int xs = x[SP] - nu(R, SP);
+        if constexpr (nu(R, SP) > 0) ok = ok && xs >= 0;
+        if constexpr (nu(R, SP) < 0) ok = ok && xs < g.dims[SP];
+        if constexpr (kind(R, SP) != 0) f *= factor<R, SP>(g, tab, min(max(xs, 0), g.dims[SP] - 1));
+        src_factor<R, SP + 1>(g, tab, x, f, ok);
+    }
+}
+
+template <int R, int SP>
+__device__ __forceinline__ void own_factor(const Regs &g, const double *__restrict__ tab, const int (&x)[NS], double &f) {
+    if constexpr (SP < NS) {
+        if constexpr (kind(R, SP) != 0) f *= factor<R, SP>(g, tab, x[SP]);
+        own_factor<R, SP + 1>(g, tab, x, f);
+    }
+}
+
+// (A v)[i] for one state: sum_r c_r (a_r(x - nu_r) v[i - d_r] 1{x - nu_r in box} - a_r(x) v[i]).
+template <int R>
+__device__ __forceinline__ void accumulate(const Regs &g, const double *__restrict__ tab, const double *__restrict__ v,
+                                           int i, const int (&x)[NS], double vi, double &acc, double &dg) {
+    if constexpr (R < NR) {
+        double fa = g.coef[R], fb = g.coef[R];
+        bool ok = true;
+        src_factor<R, 0>(g, tab, x, fa, ok);
+        own_factor<R, 0>(g, tab, x, fb);
+        const double src = ok ? __ldg(v + i - g.delta[R]) : 0.0;
+        acc = fma(ok ? fa : 0.0, src, acc);
+        dg += fb;
+        accumulate<R + 1>(g, tab, v, i, x, vi, acc, dg);
+    }
+}
+
+__device__ __forceinline__ void decode(const Regs &g, int i, int (&x)[NS]) {
+    unsigned rem = (unsigned)i;
+#pragma unroll
+    for (int sp = 0; sp < NS - 1; ++sp) {
+        const unsigned q = fdiv(rem, g.div[sp]);
+        x[sp] = (int)(rem - q * (unsigned)g.dims[sp]);
+        rem = q;
+    }
+    x[NS - 1] = (int)rem;
+}
+
+// rho * (A v)[i]
+__device__ __forceinline__ double apply_at(const Regs &g, const double *__restrict__ tab, const double *__restrict__ v,
+                                           int i, double rho) {
+    int x[NS];
+    decode(g, i, x);
+    const double vi = __ldg(v + i);
+    double acc = 0.0, dg = 0.0;
+    accumulate<0>(g, tab, v, i, x, vi, acc, dg);
+    return rho * fma(-dg, vi, acc);
+}
+
+// Warp partial sums of up to 8 values into s.warp_part[warp][k0 + k].
+__device__ __forceinline__ void warp_partials8(Shared &s, const double (&acc)[8], int k0, int kused) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-    for (int k = 0; k < K; ++k) {
-        if (k < kused) {
+    for (int k = 0; k < 8; ++k) {
+        if (k0 + k < kused) {
             double v = acc[k];
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            if (lane == 0) s.warp_part[warp][k] = v;
+            if (lane == 0) s.warp_part[warp][k0 + k] = v;
         }
     }
+}
+
+// CTA totals of s.warp_part[.][0..kused) into s.red[buf], one cluster barrier, then every CTA sums
+// the partials of all CTAs in rank order into s.tot.
+__device__ __forceinline__ void cluster_finish(cg::cluster_group &cl, Shared &s, int kused, int &buf) {
     __syncthreads();
     for (int k = threadIdx.x; k < kused; k += T) {
         double v = 0.0;
@@ -139,59 +237,10 @@ __device__ __forceinline__ void cluster_sum(cg::cluster_group &cl, Shared &s, do
     buf ^= 1;
 }
 
-// Factor f_{r,s}(x) of the current instance.
-template <int R, int SP>
-__device__ __forceinline__ double factor(const Shared &s, const double *__restrict__ tab, int x) {
-    if constexpr (kind(R, SP) == 0) return 1.0;
-    else if constexpr (kind(R, SP) == 1) return (double)x;
-    else return __ldg(tab + R * s.in.tab_stride + s.in.tab_off[SP] + x);
-}
-
-template <int R, int SP>
-__device__ __forceinline__ void src_factor(const Shared &s, const double *__restrict__ tab, const int (&x)[NS],
-                                           double &f, bool &ok) {
-    if constexpr (SP < NS) {
-        const int xs = x[SP] - nu(R, SP);
-        if constexpr (nu(R, SP) != 0) ok = ok && xs >= 0 && xs < s.in.dims[SP];
-        if constexpr (kind(R, SP) != 0) f *= factor<R, SP>(s, tab, min(max(xs, 0), s.in.dims[SP] - 1));
-        src_factor<R, SP + 1>(s, tab, x, f, ok);
-    }
-}
-
-template <int R, int SP>
-__device__ __forceinline__ void own_factor(const Shared &s, const double *__restrict__ tab, const int (&x)[NS],
-                                           double &f) {
-    if constexpr (SP < NS) {
-        if constexpr (kind(R, SP) != 0) f *= factor<R, SP>(s, tab, x[SP]);
-        own_factor<R, SP + 1>(s, tab, x, f);
-    }
-}
-
-// (A v)[i] for one state: sum_r c_r (a_r(x - nu_r) v[i - d_r] 1{x - nu_r in box} - a_r(x) v[i]).
-template <int R>
-__device__ __forceinline__ void accumulate(const Shared &s, const double *__restrict__ tab, const double *__restrict__ v,
-                                           int i, const int (&x)[NS], double vi, double &acc) {
-    if constexpr (R < NR) {
-        double fa = s.in.coef[R], fb = s.in.coef[R];
-        bool ok = true;
-        src_factor<R, 0>(s, tab, x, fa, ok);
-        own_factor<R, 0>(s, tab, x, fb);
-        const double src = ok ? v[i - s.in.delta[R]] : 0.0;
-        acc = fma(ok ? fa : 0.0, src, acc);
-        acc = fma(-fb, vi, acc);
-        accumulate<R + 1>(s, tab, v, i, x, vi, acc);
-    }
-}
-
-__device__ __forceinline__ void decode(const Shared &s, int i, int (&x)[NS]) {
-    unsigned rem = (unsigned)i;
-#pragma unroll
-    for (int sp = 0; sp < NS - 1; ++sp) {
-        const unsigned q = fdiv(rem, s.in.div[sp]);
-        x[sp] = (int)(rem - q * (unsigned)s.in.dims[sp]);
-        rem = q;
-    }
-    x[NS - 1] = (int)rem;
+__device__ __forceinline__ void cluster_sum1(cg::cluster_group &cl, Shared &s, double v, int &buf) {
+    double acc[8] = {v, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    warp_partials8(s, acc, 0, 1);
+    cluster_finish(cl, s, 1, buf);
 }
 
 // ---- small dense kernels for the (m+2)^2 exponential (column-major, k = MP2) -------------------
@@ -351,6 +400,8 @@ __device__ void solve_instance(const CufspBatchArgs &a, cg::cluster_group &cl, S
     double t_now = 0.0, t_new = 0.0, xm = 1.0 / M, err_loc = 0.0;
     const double btol = a.anorm * a.tol;
     int steps = 0, rejects = 0, matvecs = 0, status = 0;
+    Regs g;
+    load_regs(s.in, g);
 
     while (t_now < a.t_final && status == 0) {
         if (steps >= a.max_steps) {
@@ -358,9 +409,9 @@ __device__ void solve_instance(const CufspBatchArgs &a, cg::cluster_group &cl, S
             break;
         }
         // beta = ||v||
-        double acc1[1] = {0.0};
-        for (int i = i0 + (int)threadIdx.x; i < i1; i += T) acc1[0] = fma(v[i], v[i], acc1[0]);
-        cluster_sum<1>(cl, s, acc1, 1, buf);
+        double acc1 = 0.0;
+        for (int i = i0 + (int)threadIdx.x; i < i1; i += T) acc1 = fma(v[i], v[i], acc1);
+        cluster_sum1(cl, s, acc1, buf);
         const double beta = sqrt(s.tot[0]);
         if (!isfinite(beta)) {
             status = 2;
@@ -388,36 +439,52 @@ __device__ void solve_instance(const CufspBatchArgs &a, cg::cluster_group &cl, S
             const double *vj = vec(j);
             double *w = vec(j + 1);
             const double rj = s.rho[j];
-            double acc[KR];
+            // generator action (own chunk; neighbours read anywhere in the instance)
+            for (int i = i0 + (int)threadIdx.x; i < i1; i += T) w[i] = apply_at(g, tab, vj, i, rj);
+            // Gram-Schmidt dots in groups of 8 (each thread re-reads only its own w entries)
+            for (int k0 = 0; k0 < K; k0 += 8) {
+                double acc[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+                const double *vb[8];
 #pragma unroll
-            for (int k = 0; k < KR; ++k) acc[k] = 0.0;
-            for (int i = i0 + (int)threadIdx.x; i < i1; i += T) {
-                int x[NS];
-                decode(s, i, x);
-                double r = 0.0;
-                accumulate<0>(s, tab, vj, i, x, vj[i], r);
-                r *= rj;
-                w[i] = r;
+                for (int k = 0; k < 8; ++k) vb[k] = vec(istart + min(k0 + k, K - 1));
+                if (K - k0 >= 8) {
+                    for (int i = i0 + (int)threadIdx.x; i < i1; i += T) {
+                        const double wi = w[i];
 #pragma unroll
-                for (int k = 0; k < KR; ++k)
-                    if (k < K) acc[k] = fma(vec(istart + k)[i], r, acc[k]);
+                        for (int k = 0; k < 8; ++k) acc[k] = fma(vb[k][i], wi, acc[k]);
+                    }
+                } else {
+                    for (int i = i0 + (int)threadIdx.x; i < i1; i += T) {
+                        const double wi = w[i];
+#pragma unroll
+                        for (int k = 0; k < 8; ++k)
+                            if (k0 + k < K) acc[k] = fma(vb[k][i], wi, acc[k]);
+                    }
+                }
+                warp_partials8(s, acc, k0, K);
             }
-            cluster_sum<KR>(cl, s, acc, K, buf);
+            cluster_finish(cl, s, K, buf);
             for (int k = threadIdx.x; k < K; k += T) {
                 const double h = s.rho[istart + k] * s.tot[k];
                 s.H[(istart + k) + j * MP2] = h;
                 s.gam[istart + k] = h * s.rho[istart + k];
             }
             __syncthreads();
-            double acc2[1] = {0.0};
+            double acc2 = 0.0;
             for (int i = i0 + (int)threadIdx.x; i < i1; i += T) {
                 double wi = w[i];
-#pragma unroll 4
-                for (int k = 0; k < K; ++k) wi = fma(-s.gam[istart + k], vec(istart + k)[i], wi);
+                int k = 0;
+                for (; k + 4 <= K; k += 4) {
+                    wi = fma(-s.gam[istart + k], vec(istart + k)[i], wi);
+                    wi = fma(-s.gam[istart + k + 1], vec(istart + k + 1)[i], wi);
+                    wi = fma(-s.gam[istart + k + 2], vec(istart + k + 2)[i], wi);
+                    wi = fma(-s.gam[istart + k + 3], vec(istart + k + 3)[i], wi);
+                }
+                for (; k < K; ++k) wi = fma(-s.gam[istart + k], vec(istart + k)[i], wi);
                 w[i] = wi;
-                acc2[0] = fma(wi, wi, acc2[0]);
+                acc2 = fma(wi, wi, acc2);
             }
-            cluster_sum<1>(cl, s, acc2, 1, buf);
+            cluster_sum1(cl, s, acc2, buf);
             const double sn = sqrt(s.tot[0]);
             ++matvecs;
             if (!isfinite(sn)) {
@@ -442,16 +509,12 @@ __device__ void solve_instance(const CufspBatchArgs &a, cg::cluster_group &cl, S
         } else {  // avnorm = ||A v_m|| (src/KryExpvFSP.cu:114-120)
             const double *vm = vec(M);
             const double rm = s.rho[M];
-            double acc3[1] = {0.0};
+            double acc3 = 0.0;
             for (int i = i0 + (int)threadIdx.x; i < i1; i += T) {
-                int x[NS];
-                decode(s, i, x);
-                double r = 0.0;
-                accumulate<0>(s, tab, vm, i, x, vm[i], r);
-                r *= rm;
-                acc3[0] = fma(r, r, acc3[0]);
+                const double r = apply_at(g, tab, vm, i, rm);
+                acc3 = fma(r, r, acc3);
             }
-            cluster_sum<1>(cl, s, acc3, 1, buf);
+            cluster_sum1(cl, s, acc3, buf);
             avnorm = sqrt(s.tot[0]);
             ++matvecs;
             if (!isfinite(avnorm)) {
