@@ -1,0 +1,390 @@
+// cufsp_adjoint.cu -- log-likelihood gradient by the adjoint method (no counterpart in the reference,
+// whose Likelihood::evaluate, src/Likelihood.cpp:8-33, has no gradient).
+//
+//   log L(c) = sum_i sum_k D_i[k] log max(1e-44, q_i[k]),  q_i = M p(t_i),  p(t) = exp(t A(c)) p0,
+//   A(c) = sum_r c_r A_r (A_r: reaction r at unit rate),  M sums each block of `block` states.
+//
+//   d log L / d c_r = int_0^T lambda(s)^T A_r p(s) ds,   lambda(T) = g_last,  lambda' = -A^T lambda,
+//   lambda jumps by g_i = M^T (D_i / q_i) at each data time t_i (0 where q_i <= 1e-44).
+//
+// Forward pass: the adaptive Krylov solve (cufsp_krylov.cu) through the data times, storing p at
+// every accepted step boundary (checkpoints) instead of the trajectory.  Backward pass, step by step
+// in reverse: the forward Arnoldi basis V, H is rebuilt from the step's checkpoint (dense output
+// p(s) = V exp((s - s0) H) beta e1 on the whole step); lambda is integrated backward over the step with
+// the transposed generator (matrix-free A^T kernel) in adaptive sub-steps, each with its own basis U, G,
+// lambda(s) = U exp((b - s) G) gamma e1.  On a sub-step [a, b] the integral is exact in the two
+// subspaces:
+//   int_a^b lambda^T A_r p ds = sum_{a', b'} W[a'][b'] u_{a'}^T A_r v_{b'},
+//   W = int_0^tau exp((tau-u) G) z_b y_a^T exp(u H^T) du  = upper-right block of
+//       exp(tau [[G, z_b y_a^T], [0, H^T]])   (Van Loan 1978),
+// and the vector part is one fused kernel: uhat_{b'} = U W[:, b'] (multi-combination), then per state x
+//   I_r += sum_{b'} v_{b'}(x) a_r(x) (uhat_{b'}(x + nu_r) 1{x + nu_r in box} - uhat_{b'}(x))
+// for all reactions at once, with a deterministic grid reduction.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "cufsp_internal.h"
+#include "cufsp_reduce.cuh"
+
+namespace cufsp {
+namespace {
+
+constexpr int kMaxB = CUFSP_MAX_KRYLOV + 1;
+
+// g = M^T (D / q) for one data time: q[k] = sum of block k of p, g[x] = D[k] / q[k] (0 if q <= 1e-44).
+__global__ void k_loglik_grad_vec(int64_t n, const double *__restrict__ p, int64_t block,
+                                  const double *__restrict__ counts, double *__restrict__ g) {
+    const int64_t nk = n / block;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nk; k += (int64_t)gridDim.x * blockDim.x) {
+        double q = 0.0;
+        for (int64_t j = 0; j < block; ++j) q += p[k * block + j];
+        const double d = counts[k];
+        const double v = (q > 1e-44 && d != 0.0) ? d / q : 0.0;
+        for (int64_t j = 0; j < block; ++j) g[k * block + j] = v;
+    }
+}
+
+__global__ void k_axpy(int64_t n, double a, const double *__restrict__ x, double *__restrict__ y) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        y[i] = fma(a, x[i], y[i]);
+}
+
+struct CombManyArgs {
+    const double *in[kMaxB];
+    double *out[kMaxB];
+    int n_in, n_out;
+    int64_t n;
+    const double *coef;  // [n_in][n_out] (device)
+};
+
+// out_b = sum_a coef[a][b] in_a for all b; the coefficient matrix is staged in shared memory.
+__global__ void __launch_bounds__(256) k_comb_many(const CombManyArgs a) {
+    __shared__ double cs[kMaxB * kMaxB];
+    for (int e = threadIdx.x; e < a.n_in * a.n_out; e += blockDim.x) cs[e] = a.coef[e];
+    __syncthreads();
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += (int64_t)gridDim.x * blockDim.x) {
+        double acc[8];
+        for (int b0 = 0; b0 < a.n_out; b0 += 8) {
+#pragma unroll
+            for (int k = 0; k < 8; ++k) acc[k] = 0.0;
+            for (int ia = 0; ia < a.n_in; ++ia) {
+                const double x = __ldg(a.in[ia] + i);
+                const double *crow = cs + ia * a.n_out + b0;
+#pragma unroll
+                for (int k = 0; k < 8; ++k)
+                    if (b0 + k < a.n_out) acc[k] = fma(crow[k], x, acc[k]);
+            }
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+                if (b0 + k < a.n_out) a.out[b0 + k][i] = acc[k];
+        }
+    }
+}
+
+struct BilinArgs {
+    const double *v[kMaxB];     // forward basis W_b (scaled by vscale[b])
+    const double *uh[kMaxB];    // uhat_b
+    double vscale[kMaxB];
+    int nb;
+    const double *tables;
+    const int *nu;              // [nr][ns] (device)
+    int n, ns, nr, tab_stride;
+    int dims[CUFSP_MAX_SPECIES];
+    int tab_off[CUFSP_MAX_SPECIES];
+    FastDiv div[CUFSP_MAX_SPECIES];
+    int delta[CUFSP_MAX_REACTIONS];
+    double *acc_out;            // [nr] accumulated (+=) by the last CTA
+    double *partials;
+    unsigned int *counter;
+};
+
+// I_r += sum_x a_r(x) sum_b v_b(x) (uhat_b(x + nu_r) 1{in box} - uhat_b(x))  for every r at once.
+__global__ void __launch_bounds__(kRedThreads) k_adj_bilinear(const BilinArgs a) {
+    __shared__ RedSmem<32> sm;
+    double acc[32];
+#pragma unroll
+    for (int r = 0; r < 32; ++r) acc[r] = 0.0;
+    const int stride = gridDim.x * blockDim.x;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride) {
+        int xs[CUFSP_MAX_SPECIES];
+        unsigned rem = (unsigned)i;
+        for (int s = 0; s < a.ns - 1; ++s) {
+            const unsigned q = fd_div(rem, a.div[s]);
+            xs[s] = (int)(rem - q * (unsigned)a.dims[s]);
+            rem = q;
+        }
+        xs[a.ns - 1] = (int)rem;
+        // diagonal part sum_b v_b(x) uhat_b(x), shared by all reactions
+        double dsum = 0.0;
+        for (int b = 0; b < a.nb; ++b) dsum = fma(a.vscale[b] * __ldg(a.v[b] + i), __ldg(a.uh[b] + i), dsum);
+#pragma unroll 1
+        for (int r = 0; r < a.nr; ++r) {
+            double f = 1.0;
+            bool ok = true;
+            const double *tr = a.tables + (size_t)r * a.tab_stride;
+            for (int s = 0; s < a.ns; ++s) {
+                f *= __ldg(tr + a.tab_off[s] + xs[s]);
+                const int t = xs[s] + __ldg(a.nu + r * a.ns + s);
+                ok = ok && t >= 0 && t < a.dims[s];
+            }
+            double osum = 0.0;
+            if (ok) {
+                const int j = i + a.delta[r];
+                for (int b = 0; b < a.nb; ++b) osum = fma(a.vscale[b] * __ldg(a.v[b] + i), __ldg(a.uh[b] + j), osum);
+            }
+            const double c = f * (osum - dsum);
+#pragma unroll
+            for (int rr = 0; rr < 32; ++rr)
+                if (rr == r) acc[rr] += c;
+        }
+    }
+    if (!grid_reduce<32>(acc, a.nr, a.partials, a.counter, sm)) return;
+    for (int r = threadIdx.x; r < a.nr; r += blockDim.x) a.acc_out[r] += sm.final_[r];
+}
+
+// beta * exp(s H) e1 for an mb x mb column-major H (host).
+cufsp_status dense_output(int mb, const std::vector<double> &H, double s, double beta, std::vector<double> &y) {
+    y.assign(mb, 0.0);
+    if (mb == 0) return CUFSP_SUCCESS;
+    std::vector<double> X((size_t)mb * mb), F((size_t)mb * mb);
+    for (size_t i = 0; i < X.size(); ++i) X[i] = s * H[i];
+    cufsp_status st = expm_pade13(mb, X.data(), F.data());
+    if (st != CUFSP_SUCCESS) return st;
+    for (int i = 0; i < mb; ++i) y[i] = beta * F[i];
+    return CUFSP_SUCCESS;
+}
+
+struct Checkpoint {
+    double *p;
+    double tau;
+};
+
+struct AdjWork {
+    std::vector<double *> bufs;
+    ~AdjWork() {
+        for (double *b : bufs) cudaFree(b);
+    }
+    double *alloc(size_t n) {
+        double *p = nullptr;
+        if (cudaMalloc(&p, sizeof(double) * n) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        bufs.push_back(p);
+        return p;
+    }
+};
+
+struct ExpvGuard {
+    cufsp_expv *E = nullptr;
+    ~ExpvGuard() {
+        if (E) cufsp_expv_destroy(E);
+    }
+};
+
+}  // namespace
+}  // namespace cufsp
+
+using namespace cufsp;
+
+extern "C" cufsp_status cufsp_likelihood_grad(cufsp_mat *A, const double *coefs, int n_times, const double *times,
+                                              const double *d_p0, int64_t block, const double *d_counts, int m,
+                                              double tol, double *logL, double *grad, cufsp_stream_t stream) {
+    clear_error();
+    if (!A || !coefs || !times || !d_p0 || !d_counts || !logL || !grad || n_times < 1)
+        return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_likelihood_grad: NULL argument");
+    if (!A->kron) return set_error(CUFSP_ERR_UNSUPPORTED, "cufsp_likelihood_grad: needs a KRONECKER generator");
+    const int64_t n = A->model.n;
+    const int nr = A->model.nr, ns = A->model.ns;
+    if (block < 1 || n % block != 0) return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_likelihood_grad: bad block");
+    if (nr > 32) return set_error(CUFSP_ERR_UNSUPPORTED, "cufsp_likelihood_grad: at most 32 reactions");
+    for (int i = 0; i < n_times; ++i)
+        if (!(times[i] >= (i ? times[i - 1] : 0.0)) || !std::isfinite(times[i]))
+            return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_likelihood_grad: times must be finite and non-decreasing");
+    cudaStream_t st = (cudaStream_t)stream;
+    std::vector<double> c(coefs, coefs + nr);
+    for (double v : c)
+        if (!std::isfinite(v)) return set_error(CUFSP_ERR_NONFINITE, "cufsp_likelihood_grad: coefficient is NaN/Inf");
+
+    ExpvGuard ef, eb;
+    cufsp_status s = cufsp_expv_create(n, m, tol, 0, 2, 1.0, &ef.E);
+    if (s == CUFSP_SUCCESS) s = cufsp_expv_create(n, m, tol, 0, 2, 1.0, &eb.E);
+    if (s == CUFSP_SUCCESS) s = cufsp_expv_bind_mat_coefs(ef.E, A, c.data());
+    if (s == CUFSP_SUCCESS) s = cufsp_expv_bind_mat_coefs(eb.E, A, c.data());
+    if (s != CUFSP_SUCCESS) return s;
+    expv_set_transpose(eb.E, true);
+
+    AdjWork wk;
+    double *p = wk.alloc(n), *lam = wk.alloc(n), *lam_b = wk.alloc(n), *pf = wk.alloc(n);
+    double *g = wk.alloc((size_t)n * n_times);
+    double *uh = wk.alloc((size_t)n * (m + 1));
+    double *d_misc = wk.alloc(64 + (size_t)kMaxB * kMaxB);  // [0..31] I_r, [32] loglik, [64..] coefficient matrix
+    ReduceScratch rs;
+    if (!p || !lam || !lam_b || !pf || !g || !uh || !d_misc)
+        return set_error(CUFSP_ERR_ALLOC, "cufsp_likelihood_grad: device allocation failed");
+    struct RsGuard {
+        ReduceScratch &r;
+        ~RsGuard() { r.release(); }
+    } rsg{rs};
+    const int red_grid = stream_grid(n, 4, device_info().sm_count * 4);
+    s = rs.init(red_grid, 32);
+    if (s != CUFSP_SUCCESS) return s;
+    double *d_I = d_misc, *d_ll = d_misc + 32, *d_coef = d_misc + 64;
+    CUFSP_CUDA_TRY(cudaMemsetAsync(d_misc, 0, sizeof(double) * 64, st));
+    const int vgrid = stream_grid(n, 4, device_info().sm_count * 8);
+
+    // ---- forward pass with checkpoints ----
+    CUFSP_CUDA_TRY(cudaMemcpyAsync(p, d_p0, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+    std::vector<std::vector<Checkpoint>> steps(n_times);
+    double ll = 0.0, t_prev = 0.0;
+    for (int i = 0; i < n_times; ++i) {
+        const double dt = times[i] - t_prev;
+        t_prev = times[i];
+        if (dt > 0.0) {
+            CUFSP_CUDA_TRY(cudaStreamSynchronize(st));
+            s = cufsp_expv_set_final_time(ef.E, dt);
+            if (s == CUFSP_SUCCESS) s = cufsp_expv_reset_time(ef.E);
+            if (s != CUFSP_SUCCESS) return s;
+            int reached = 0;
+            while (!reached) {
+                double *ck = wk.alloc(n);
+                if (!ck) return set_error(CUFSP_ERR_ALLOC, "cufsp_likelihood_grad: checkpoint allocation failed");
+                CUFSP_CUDA_TRY(cudaMemcpyAsync(ck, p, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+                s = expv_step_once(ef.E, p, st);
+                if (s != CUFSP_SUCCESS) return s;
+                steps[i].push_back({ck, expv_last(ef.E).tau});
+                cufsp_expv_final_time_reached(ef.E, &reached);
+            }
+        }
+        double li = 0.0;
+        s = cufsp_loglik(n, p, block, d_counts + (size_t)i * (n / block), &li, stream);
+        if (s != CUFSP_SUCCESS) return s;
+        ll += li;
+        k_loglik_grad_vec<<<vgrid, 256, 0, st>>>(n, p, block, d_counts + (size_t)i * (n / block), g + (size_t)i * n);
+        CUFSP_CUDA_TRY(cudaGetLastError());
+    }
+
+    // ---- backward pass ----
+    CUFSP_CUDA_TRY(cudaMemsetAsync(lam, 0, sizeof(double) * n, st));
+    BilinArgs ba;
+    std::memset(&ba, 0, sizeof(ba));
+    ba.tables = nullptr;
+    const ModelHost &mh = A->model;
+    // device copies of the model tables / stoichiometry for the bilinear kernel
+    double *d_tab = wk.alloc(mh.tables.size());
+    double *d_nu_d = wk.alloc((mh.nu.size() + 1) / 2 + 1);  // int storage inside a double buffer
+    if (!d_tab || !d_nu_d) return set_error(CUFSP_ERR_ALLOC, "cufsp_likelihood_grad: device allocation failed");
+    CUFSP_CUDA_TRY(cudaMemcpyAsync(d_tab, mh.tables.data(), sizeof(double) * mh.tables.size(), cudaMemcpyHostToDevice, st));
+    CUFSP_CUDA_TRY(cudaMemcpyAsync(d_nu_d, mh.nu.data(), sizeof(int) * mh.nu.size(), cudaMemcpyHostToDevice, st));
+    ba.tables = d_tab;
+    ba.nu = reinterpret_cast<const int *>(d_nu_d);
+    ba.n = (int)n;
+    ba.ns = ns;
+    ba.nr = nr;
+    ba.tab_stride = mh.tab_stride;
+    {
+        int64_t stride = 1;
+        for (int sp = 0; sp < ns; ++sp) {
+            ba.dims[sp] = mh.bounds[sp] + 1;
+            ba.tab_off[sp] = mh.tab_off[sp];
+            ba.div[sp] = make_fastdiv((uint32_t)ba.dims[sp]);
+            stride *= ba.dims[sp];
+        }
+        for (int r = 0; r < nr; ++r) {
+            int64_t d = 0, stv = 1;
+            for (int sp = 0; sp < ns; ++sp) {
+                d += (int64_t)mh.nu[(size_t)r * ns + sp] * stv;
+                stv *= ba.dims[sp];
+            }
+            ba.delta[r] = (int)std::max<int64_t>(-n, std::min<int64_t>(n, d));
+        }
+    }
+    ba.acc_out = d_I;
+    ba.partials = rs.partials;
+    ba.counter = rs.counter;
+
+    std::vector<double> ya, Xb, Fb, coefm;
+    for (int i = n_times - 1; i >= 0; --i) {
+        k_axpy<<<vgrid, 256, 0, st>>>(n, 1.0, g + (size_t)i * n, lam);
+        CUFSP_CUDA_TRY(cudaGetLastError());
+        double s_end = times[i];  // end of the current forward step
+        for (int k = (int)steps[i].size() - 1; k >= 0; --k) {
+            const Checkpoint &ck = steps[i][k];
+            const double h = ck.tau;
+            const double s0 = s_end - h;
+            // forward basis on this step from its checkpoint
+            CUFSP_CUDA_TRY(cudaMemcpyAsync(pf, ck.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+            s = expv_arnoldi(ef.E, pf, st);
+            if (s != CUFSP_SUCCESS) return s;
+            const KrylovStep F = expv_last(ef.E);
+            // lambda backward over [s0, s_end] in adaptive sub-steps
+            CUFSP_CUDA_TRY(cudaStreamSynchronize(st));
+            s = cufsp_expv_set_final_time(eb.E, h);
+            if (s == CUFSP_SUCCESS) s = cufsp_expv_reset_time(eb.E);
+            if (s != CUFSP_SUCCESS) return s;
+            double b_end = s_end;
+            int reached = h <= 0.0;
+            while (!reached) {
+                CUFSP_CUDA_TRY(cudaMemcpyAsync(lam_b, lam, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+                s = expv_step_once(eb.E, lam, st);
+                if (s != CUFSP_SUCCESS) return s;
+                const KrylovStep B = expv_last(eb.E);
+                cufsp_expv_final_time_reached(eb.E, &reached);
+                const double tau = B.tau;
+                const double a0 = b_end - tau;
+                if (F.beta > 0.0 && B.beta > 0.0 && tau > 0.0) {
+                    // W = upper-right mb_b x mb_f block of exp(tau [[G, z_b y_a^T], [0, H^T]])
+                    s = dense_output(F.mb, F.H, a0 - s0, F.beta, ya);
+                    if (s != CUFSP_SUCCESS) return s;
+                    const int mbb = B.mb, mbf = F.mb, K = mbb + mbf;
+                    Xb.assign((size_t)K * K, 0.0);
+                    Fb.assign((size_t)K * K, 0.0);
+                    for (int jj = 0; jj < mbb; ++jj)
+                        for (int ii = 0; ii < mbb; ++ii) Xb[ii + (size_t)jj * K] = tau * B.H[ii + (size_t)jj * mbb];
+                    for (int jj = 0; jj < mbf; ++jj) Xb[0 + (size_t)(mbb + jj) * K] = tau * B.beta * ya[jj];
+                    for (int jj = 0; jj < mbf; ++jj)
+                        for (int ii = 0; ii < mbf; ++ii)
+                            Xb[(mbb + ii) + (size_t)(mbb + jj) * K] = tau * F.H[jj + (size_t)ii * mbf];  // H^T
+                    s = expm_pade13(K, Xb.data(), Fb.data());
+                    if (s != CUFSP_SUCCESS) return s;
+                    // uhat_b = sum_a W[a][b] rho_b[a] Ub_a
+                    coefm.assign((size_t)mbb * mbf, 0.0);
+                    for (int aa = 0; aa < mbb; ++aa)
+                        for (int bb = 0; bb < mbf; ++bb)
+                            coefm[(size_t)aa * mbf + bb] = Fb[aa + (size_t)(mbb + bb) * K] * B.rho[aa];
+                    CUFSP_CUDA_TRY(cudaMemcpyAsync(d_coef, coefm.data(), sizeof(double) * coefm.size(),
+                                                   cudaMemcpyHostToDevice, st));
+                    CombManyArgs ca;
+                    ca.n_in = mbb;
+                    ca.n_out = mbf;
+                    ca.n = n;
+                    ca.coef = d_coef;
+                    for (int aa = 0; aa < mbb; ++aa) ca.in[aa] = expv_basis(eb.E, lam_b, aa);
+                    for (int bb = 0; bb < mbf; ++bb) ca.out[bb] = uh + (size_t)bb * n;
+                    k_comb_many<<<vgrid, 256, 0, st>>>(ca);
+                    CUFSP_CUDA_TRY(cudaGetLastError());
+                    ba.nb = mbf;
+                    for (int bb = 0; bb < mbf; ++bb) {
+                        ba.v[bb] = expv_basis(ef.E, pf, bb);
+                        ba.vscale[bb] = F.rho[bb];
+                        ba.uh[bb] = uh + (size_t)bb * n;
+                    }
+                    k_adj_bilinear<<<red_grid, kRedThreads, 0, st>>>(ba);
+                    CUFSP_CUDA_TRY(cudaGetLastError());
+                    CUFSP_CUDA_TRY(cudaStreamSynchronize(st));  // d_coef / uh are reused by the next sub-step
+                }
+                b_end = a0;
+            }
+            s_end = s0;
+        }
+    }
+    std::vector<double> I(nr);
+    CUFSP_CUDA_TRY(cudaMemcpyAsync(I.data(), d_I, sizeof(double) * nr, cudaMemcpyDeviceToHost, st));
+    CUFSP_CUDA_TRY(cudaStreamSynchronize(st));
+    (void)d_ll;
+    *logL = ll;
+    for (int r = 0; r < nr; ++r) grad[r] = c[r] * I[r];  // d log L / d log c_r
+    return CUFSP_SUCCESS;
+}

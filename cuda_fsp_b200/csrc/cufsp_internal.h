@@ -130,8 +130,25 @@ int plane_watchdog(PlaneData *pd);         // 1 if a bounded barrier wait expire
 bool plane_launch(PlaneData *pd, const double *coefs, double alpha, const double *d_alpha, const int *d_skip,
                   const double *x, bool accumulate, double *y, cudaStream_t st, int64_t i_begin, int64_t i_end,
                   cufsp_status *status);
+// Coefficient-dependent tables of the plane kernel (row words), rebuilt when the coefficients change.
+cufsp_status plane_prepare(PlaneData *pd, const double *coefs, cudaStream_t st);
+cufsp_status kron_prepare(KronData *k, const double *coefs, cudaStream_t st);
 // Human-readable kernel choice of a KRONECKER generator.
 std::string kron_describe(const KronData *k);
+
+// Transposed generator action y = alpha * A(coefs)^T x (overwrite), KRONECKER format
+// (cufsp_adjoint.cu); d_alpha / d_skip as in kron_apply.
+cufsp_status kron_apply_transpose(KronData *k, const double *coefs, double alpha, const double *d_alpha,
+                                  const int *d_skip, const double *x, double *y, cudaStream_t st);
+
+// Basis data of one Arnoldi pass (single-instance Krylov driver, cufsp_krylov.cu), for the adjoint.
+struct KrylovStep {
+    int mb = 0;               // basis size (m, or the happy-breakdown size)
+    double beta = 0.0;        // ||v||
+    double tau = 0.0;         // accepted step length (expv_step), 0 after a bare Arnoldi pass
+    std::vector<double> H;    // leading mb x mb Hessenberg block, column-major
+    std::vector<double> rho;  // v_k = rho_k W_k
+};
 
 // Host-side dense exponential (cufsp_expm.cpp).
 cufsp_status expm_pade13(int k, const double *A, double *F);
@@ -157,4 +174,17 @@ cufsp_status mat_apply(cufsp_mat *A, const double *coefs, double alpha, const do
                        const double *x, bool accumulate, double *y, cudaStream_t st, int64_t i_begin = 0,
                        int64_t i_end = -1);
 cufsp_status mat_coefs(cufsp_mat *A, double t, const double *coefs_in, std::vector<double> &out);
+// Bring the generator's coefficient-dependent device tables up to `coefs` (stream order); applies
+// captured in a CUDA graph after this call launch nothing else.
+cufsp_status mat_prepare(cufsp_mat *A, const double *coefs, cudaStream_t st);
+// y = alpha * A(coefs)^T x (overwrite); KRONECKER generators only.
+cufsp_status mat_apply_transpose(cufsp_mat *A, const double *coefs, double alpha, const double *d_alpha,
+                                 const int *d_skip, const double *x, double *y, cudaStream_t st);
+
+// Internals of the single-instance Krylov driver used by the adjoint gradient (cufsp_krylov.cu).
+void expv_set_transpose(cufsp_expv *E, bool transpose);
+cufsp_status expv_arnoldi(cufsp_expv *E, double *v, cudaStream_t st);  // Arnoldi pass only
+cufsp_status expv_step_once(cufsp_expv *E, double *v, cudaStream_t st);  // one accepted step
+const KrylovStep &expv_last(const cufsp_expv *E);
+const double *expv_basis(const cufsp_expv *E, const double *v, int k);  // W_k (W_0 = v)
 }  // namespace cufsp

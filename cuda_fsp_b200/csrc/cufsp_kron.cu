@@ -671,10 +671,89 @@ int kron_watchdog(KronData *k) {
 int64_t kron_halo(const KronData *k) { return k->plane ? std::max<int64_t>(k->halo, plane_size(k->plane)) : k->halo; }
 int64_t kron_row_len(const KronData *k) { return k->plane ? plane_size(k->plane) : k->L; }
 
+cufsp_status kron_prepare(KronData *k, const double *coefs, cudaStream_t st) {
+    return k->plane ? plane_prepare(k->plane, coefs, st) : CUFSP_SUCCESS;
+}
+
 std::string kron_describe(const KronData *k) {
     if (k->plane) return plane_description(k->plane);
     return "k_kron_mv (NR=" + std::to_string(k->NR) + " NG=" + std::to_string(k->NG) + " V=" + std::to_string(k->V) +
            " inner species=" + std::to_string(k->k) + "); plane kernel not used: " + k->plane_why;
+}
+
+// ---- transposed action (adjoint solves) ---------------------------------------------------------
+// (A^T l)(x) = sum_r c_r a_r(x) (l[x + nu_r] 1{x + nu_r in box} - l[x]): the column of the generator
+// at state x (outflow a_r(x) to x + nu_r, or out of the box) read as a row.  One thread per state,
+// factors from the tables; used by the adjoint gradient, not on the forward hot path.
+struct KronTArgs {
+    const double *__restrict__ tables;
+    const int *__restrict__ nu;  // [NR][ns]
+    const double *__restrict__ d_alpha;
+    const int *__restrict__ d_skip;
+    int n, ns, nr, tab_stride;
+    int dims[CUFSP_MAX_SPECIES];
+    int tab_off[CUFSP_MAX_SPECIES];
+    FastDiv div[CUFSP_MAX_SPECIES];
+    int delta[CUFSP_MAX_REACTIONS];
+    double coef[CUFSP_MAX_REACTIONS];
+};
+
+__global__ void __launch_bounds__(256) k_kron_mvT(const KronTArgs a, const double *__restrict__ x, double *__restrict__ y) {
+    if (a.d_skip && *a.d_skip) return;
+    const double alpha = a.d_alpha ? __ldg(a.d_alpha) : 1.0;
+    const int stride = gridDim.x * blockDim.x;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride) {
+        int xs[CUFSP_MAX_SPECIES];
+        unsigned rem = (unsigned)i;
+        for (int s = 0; s < a.ns - 1; ++s) {
+            const unsigned q = fd_div(rem, a.div[s]);
+            xs[s] = (int)(rem - q * (unsigned)a.dims[s]);
+            rem = q;
+        }
+        xs[a.ns - 1] = (int)rem;
+        const double xi = __ldg(x + i);
+        double acc = 0.0;
+        for (int r = 0; r < a.nr; ++r) {
+            double f = a.coef[r];
+            bool ok = true;
+            const double *tr = a.tables + (size_t)r * a.tab_stride;
+            for (int s = 0; s < a.ns; ++s) {
+                f *= __ldg(tr + a.tab_off[s] + xs[s]);
+                const int t = xs[s] + __ldg(a.nu + r * a.ns + s);
+                ok = ok && t >= 0 && t < a.dims[s];
+            }
+            const double tgt = ok ? __ldg(x + i + a.delta[r]) : 0.0;
+            acc = fma(f, tgt - xi, acc);
+        }
+        y[i] = alpha * acc;
+    }
+}
+
+cufsp_status kron_apply_transpose(KronData *kd, const double *coefs, double alpha, const double *d_alpha,
+                                  const int *d_skip, const double *x, double *y, cudaStream_t st) {
+    KronTArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.tables = kd->d_tables;
+    a.nu = kd->d_nu;
+    a.d_alpha = d_alpha;
+    a.d_skip = d_skip;
+    a.n = (int)kd->n;
+    a.ns = kd->ns;
+    a.nr = kd->nr;
+    a.tab_stride = kd->tab_stride;
+    for (int s = 0; s < kd->ns; ++s) {
+        a.dims[s] = kd->dims[s];
+        a.tab_off[s] = kd->tab_off[s];
+        a.div[s] = make_fastdiv((uint32_t)kd->dims[s]);
+    }
+    for (int r = 0; r < kd->nr; ++r) {
+        a.delta[r] = kd->delta[r];
+        a.coef[r] = alpha * coefs[r];
+    }
+    const int grid = (int)std::min<int64_t>((kd->n + 255) / 256, (int64_t)device_info().sm_count * 16);
+    k_kron_mvT<<<std::max(grid, 1), 256, 0, st>>>(a, x, y);
+    CUFSP_CUDA_TRY(cudaGetLastError());
+    return CUFSP_SUCCESS;
 }
 
 cufsp_status kron_apply(KronData *kd, const double *coefs, double alpha, const double *d_alpha, const int *d_skip,

@@ -382,6 +382,23 @@ int plane_watchdog(PlaneData *pd) {
     return v;
 }
 
+// Row words for these coefficients, rebuilt in stream order when they change.
+cufsp_status plane_prepare(PlaneData *pd, const double *coefs, cudaStream_t st) {
+    std::vector<double> cv(coefs, coefs + pd->nr);
+    if (cv == pd->words_coefs) return CUFSP_SUCCESS;
+    for (int r = 0; r < pd->nr; ++r) pd->wa.coef[r] = cv[r];
+    const int64_t rows = (int64_t)pd->n1 * pd->n2;
+    const int64_t tot = rows * pd->wa.nwp;
+    k_plane_words<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(pd->wa, pd->d_gtab, rows, pd->d_words);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        pd->words_coefs.clear();
+        return cuda_error(e, "plane row words");
+    }
+    pd->words_coefs = cv;
+    return CUFSP_SUCCESS;
+}
+
 bool plane_launch(PlaneData *pd, const double *coefs, double alpha, const double *d_alpha, const int *d_skip,
                   const double *x, bool accumulate, double *y, cudaStream_t st, int64_t i_begin, int64_t i_end,
                   cufsp_status *status) {
@@ -393,20 +410,12 @@ bool plane_launch(PlaneData *pd, const double *coefs, double alpha, const double
     *status = CUFSP_SUCCESS;
     const int zb = (int)(i_begin / P), ze = (int)(i_end / P);
     if (ze <= zb) return true;
-    // row words for these coefficients (rebuilt in stream order when they change)
-    std::vector<double> cv(coefs, coefs + pd->nr);
-    if (cv != pd->words_coefs) {
-        for (int r = 0; r < pd->nr; ++r) pd->wa.coef[r] = cv[r];
-        const int64_t rows = (int64_t)pd->n1 * pd->n2;
-        const int64_t tot = rows * pd->wa.nwp;
-        k_plane_words<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(pd->wa, pd->d_gtab, rows, pd->d_words);
-        const cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) {
-            pd->words_coefs.clear();
-            *status = cuda_error(e, "plane row words");
+    {
+        const cufsp_status ws = plane_prepare(pd, coefs, st);
+        if (ws != CUFSP_SUCCESS) {
+            *status = ws;
             return true;
         }
-        pd->words_coefs = cv;
     }
     CufspPlaneArgs a;
     std::memset(&a, 0, sizeof(a));

@@ -19,6 +19,7 @@
 // exact (:48), a zero vector is returned unchanged, NaN/Inf and exhausted limits return errors.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "cufsp_internal.h"
@@ -198,6 +199,16 @@ struct cufsp_expv_s {
     int grid = 1;
     std::vector<double> hstate, Hh, F, tH;
     cufsp_expv_stats stats;
+    bool transpose = false;      // apply A^T instead of A (adjoint solves)
+    cufsp::KrylovStep last;      // basis data of the last Arnoldi pass / accepted step
+    // CUDA graphs of the Arnoldi pass (generator-bound operators only), one per (vector, form)
+    struct Graph {
+        const double *v;
+        bool avnorm, transpose;
+        cudaGraphExec_t exec;
+    };
+    std::vector<Graph> graphs;
+    cudaStream_t cap_stream = nullptr;
 };
 
 namespace {
@@ -205,6 +216,7 @@ namespace {
 inline double *wvec(cufsp_expv *E, double *v, int k) { return k == 0 ? v : E->W + (size_t)(k - 1) * E->n; }
 
 cufsp_status matvec(cufsp_expv *E, const double *x, double *y, const double *d_alpha, cudaStream_t st) {
+    if (E->A && E->transpose) return mat_apply_transpose(E->A, E->coefs.data(), 1.0, d_alpha, E->ks.flag, x, y, st);
     if (E->A) return mat_apply(E->A, E->coefs.data(), 1.0, d_alpha, E->ks.flag, x, false, y, st);
     // MVFun form (src/KryExpvFSP.h:15): the callback accumulates into a zeroed y.
     cufsp_status s = launch_fill(E->n, y, 0.0, st);
@@ -247,6 +259,98 @@ cufsp_status arnoldi_dot_update(cufsp_expv *E, double *v, int j, int istart, cud
     return CUFSP_SUCCESS;
 }
 
+// The Arnoldi pass of one step, entirely on the device (src/KryExpvFSP.cu:38-120): basis
+// W_1..W_{m+1} (W_0 = v), Hessenberg matrix, rho, beta, ||A v_m|| (when with_avnorm), breakdown
+// flag; one device->host copy of the state block into E->hstate.
+// The launches of one Arnoldi pass on stream st (no synchronisation).
+cufsp_status arnoldi_launches(cufsp_expv *E, double *v, cudaStream_t st, bool with_avnorm) {
+    const int m = E->m;
+    k_step_begin<<<E->grid, kRedThreads, 0, st>>>(E->n, v, E->ks, E->rs.partials, E->rs.counter);
+    CUFSP_CUDA_TRY(cudaGetLastError());
+    cufsp_status s;
+    int istart = 0;
+    for (int j = 0; j < m; ++j) {
+        s = matvec(E, wvec(E, v, j), wvec(E, v, j + 1), E->ks.rho + j, st);
+        if (s != CUFSP_SUCCESS) return s;
+        if (E->iop) istart = (j >= E->q_iop - 1) ? j - E->q_iop + 1 : 0;
+        s = arnoldi_dot_update(E, v, j, istart, st);
+        if (s != CUFSP_SUCCESS) return s;
+    }
+    if (with_avnorm) {
+        s = matvec(E, wvec(E, v, m), wvec(E, v, m + 1), E->ks.rho + m, st);
+        if (s != CUFSP_SUCCESS) return s;
+        k_avnorm<<<E->grid, kRedThreads, 0, st>>>(E->n, wvec(E, v, m + 1), E->ks, E->rs.partials, E->rs.counter);
+        CUFSP_CUDA_TRY(cudaGetLastError());
+    }
+    return CUFSP_SUCCESS;
+}
+
+bool graphs_enabled() {
+    static const bool on = [] {
+        const char *e = getenv("CUFSP_KRYLOV_GRAPH");
+        return !e || atoi(e) != 0;
+    }();
+    return on;
+}
+
+// The Arnoldi pass of one step, entirely on the device (src/KryExpvFSP.cu:38-120): basis
+// W_1..W_{m+1} (W_0 = v), Hessenberg matrix, rho, beta, ||A v_m|| (when with_avnorm), breakdown
+// flag; one device->host copy of the state block into E->hstate.  With a generator bound, the ~3m
+// launches are captured once per (vector, form) into a CUDA graph and replayed (one launch per
+// step); the generator's coefficient-dependent tables are prepared eagerly before each replay.
+cufsp_status arnoldi_pass(cufsp_expv *E, double *v, cudaStream_t st, bool with_avnorm) {
+    cufsp_status s;
+    if (E->A && graphs_enabled()) {
+        s = mat_prepare(E->A, E->coefs.data(), st);
+        if (s != CUFSP_SUCCESS) return s;
+        cudaGraphExec_t exec = nullptr;
+        for (auto &g : E->graphs)
+            if (g.v == v && g.avnorm == with_avnorm && g.transpose == E->transpose) exec = g.exec;
+        if (!exec) {
+            if (!E->cap_stream) CUFSP_CUDA_TRY(cudaStreamCreateWithFlags(&E->cap_stream, cudaStreamNonBlocking));
+            cudaGraph_t graph = nullptr;
+            CUFSP_CUDA_TRY(cudaStreamBeginCapture(E->cap_stream, cudaStreamCaptureModeThreadLocal));
+            s = arnoldi_launches(E, v, E->cap_stream, with_avnorm);
+            const cudaError_t e = cudaStreamEndCapture(E->cap_stream, &graph);
+            if (s != CUFSP_SUCCESS) {
+                if (graph) cudaGraphDestroy(graph);
+                return s;
+            }
+            if (e != cudaSuccess) return cuda_error(e, "expv: graph capture");
+            const cudaError_t e2 = cudaGraphInstantiate(&exec, graph, 0);
+            cudaGraphDestroy(graph);
+            if (e2 != cudaSuccess) return cuda_error(e2, "expv: graph instantiate");
+            if (E->graphs.size() >= 4) {  // a small cache; the oldest entry goes
+                cudaGraphExecDestroy(E->graphs.front().exec);
+                E->graphs.erase(E->graphs.begin());
+            }
+            E->graphs.push_back({v, with_avnorm, E->transpose, exec});
+        }
+        CUFSP_CUDA_TRY(cudaGraphLaunch(exec, st));
+    } else {
+        s = arnoldi_launches(E, v, st, with_avnorm);
+        if (s != CUFSP_SUCCESS) return s;
+    }
+    const int m = E->m;
+    CUFSP_CUDA_TRY(cudaMemcpyAsync(E->hstate.data(), E->d_state, E->state_bytes, cudaMemcpyDeviceToHost, st));
+    CUFSP_CUDA_TRY(cudaStreamSynchronize(st));
+    // basis data for the adjoint (leading mb x mb block of H, rho, beta)
+    const int mp2 = m + 2;
+    const double *hH = E->hstate.data();
+    const double *hrho = hH + (size_t)mp2 * mp2;
+    int flag;
+    std::memcpy(&flag, hrho + 2 * mp2 + 4, sizeof(int));
+    KrylovStep &L = E->last;
+    L.mb = flag > 0 ? flag : m;
+    L.beta = hrho[2 * mp2];
+    L.H.assign((size_t)L.mb * L.mb, 0.0);
+    for (int j = 0; j < L.mb; ++j)
+        for (int i = 0; i < L.mb; ++i) L.H[i + (size_t)j * L.mb] = hH[i + (size_t)j * mp2];
+    L.rho.assign(hrho, hrho + L.mb);
+    L.tau = 0.0;
+    return CUFSP_SUCCESS;
+}
+
 double round2(double t) {
     const double s = std::pow(10.0, std::floor(std::log10(t)) - 1.0);
     return std::ceil(t / s) * s;
@@ -260,25 +364,8 @@ cufsp_status expv_step(cufsp_expv *E, double *v, cudaStream_t st) {
     const double delta = 1.2, gamma = 0.9;
     if (E->i_step == 0) E->btol = E->anorm * E->tol;  // tolerance for happy breakdown (:50)
 
-    // ---- Arnoldi pass, entirely on the device ----
-    k_step_begin<<<E->grid, kRedThreads, 0, st>>>(E->n, v, E->ks, E->rs.partials, E->rs.counter);
-    CUFSP_CUDA_TRY(cudaGetLastError());
-    cufsp_status s;
-    int istart = 0;
-    for (int j = 0; j < m; ++j) {
-        s = matvec(E, wvec(E, v, j), wvec(E, v, j + 1), E->ks.rho + j, st);
-        if (s != CUFSP_SUCCESS) return s;
-        if (E->iop) istart = (j >= E->q_iop - 1) ? j - E->q_iop + 1 : 0;
-        s = arnoldi_dot_update(E, v, j, istart, st);
-        if (s != CUFSP_SUCCESS) return s;
-    }
-    s = matvec(E, wvec(E, v, m), wvec(E, v, m + 1), E->ks.rho + m, st);
+    cufsp_status s = arnoldi_pass(E, v, st, true);
     if (s != CUFSP_SUCCESS) return s;
-    k_avnorm<<<E->grid, kRedThreads, 0, st>>>(E->n, wvec(E, v, m + 1), E->ks, E->rs.partials, E->rs.counter);
-    CUFSP_CUDA_TRY(cudaGetLastError());
-    CUFSP_CUDA_TRY(cudaMemcpyAsync(E->hstate.data(), E->d_state, E->state_bytes, cudaMemcpyDeviceToHost, st));
-    CUFSP_CUDA_TRY(cudaStreamSynchronize(st));
-
     const double *hH = E->hstate.data();
     const double *hrho = hH + (size_t)mp2 * mp2;
     const double beta = hrho[2 * mp2];
@@ -287,6 +374,8 @@ cufsp_status expv_step(cufsp_expv *E, double *v, cudaStream_t st) {
     std::memcpy(&flag, hrho + 2 * mp2 + 4, sizeof(int));
     if (flag == -2) {  // zero vector: exp(tA) 0 = 0
         E->t_now = E->t_final;
+        E->last.tau = 0.0;
+        E->last.beta = 0.0;
         return CUFSP_SUCCESS;
     }
     if (flag == -1) return set_error(CUFSP_ERR_NONFINITE, "expv: NaN/Inf in the Krylov iteration");
@@ -364,6 +453,7 @@ cufsp_status expv_step(cufsp_expv *E, double *v, cudaStream_t st) {
     CUFSP_CUDA_TRY(cudaGetLastError());
 
     const bool last = (tau >= E->t_final - E->t_now);
+    E->last.tau = last ? E->t_final - E->t_now : tau;
     E->t_now = last ? E->t_final : E->t_now + tau;
     if (err_loc > 0.0) E->t_new = round2(gamma * tau * std::pow(tau * E->tol / err_loc, E->xm));
     if (!(E->t_new > 0.0) || !std::isfinite(E->t_new)) E->t_new = E->t_final - E->t_now;
@@ -375,6 +465,16 @@ cufsp_status expv_step(cufsp_expv *E, double *v, cudaStream_t st) {
 }
 
 }  // namespace
+
+namespace cufsp {
+void expv_set_transpose(cufsp_expv *E, bool transpose) { E->transpose = transpose; }
+cufsp_status expv_arnoldi(cufsp_expv *E, double *v, cudaStream_t st) { return arnoldi_pass(E, v, st, false); }
+cufsp_status expv_step_once(cufsp_expv *E, double *v, cudaStream_t st) { return expv_step(E, v, st); }
+const KrylovStep &expv_last(const cufsp_expv *E) { return E->last; }
+const double *expv_basis(const cufsp_expv *E, const double *v, int k) {
+    return k == 0 ? v : E->W + (size_t)(k - 1) * E->n;
+}
+}  // namespace cufsp
 
 extern "C" cufsp_status cufsp_expv_create(int64_t n, int m, double tol, int iop, int q_iop, double anorm,
                                           cufsp_expv **out) {
@@ -427,6 +527,8 @@ extern "C" cufsp_status cufsp_expv_create(int64_t n, int m, double tol, int iop,
 
 extern "C" cufsp_status cufsp_expv_destroy(cufsp_expv *E) {
     if (!E) return CUFSP_SUCCESS;
+    for (auto &g : E->graphs) cudaGraphExecDestroy(g.exec);
+    if (E->cap_stream) cudaStreamDestroy(E->cap_stream);
     if (E->W) cudaFree(E->W);
     if (E->d_state) cudaFree(E->d_state);
     E->rs.release();
@@ -448,6 +550,9 @@ extern "C" cufsp_status cufsp_expv_bind_mat_coefs(cufsp_expv *E, cufsp_mat *A, c
     if (n != E->n) return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_expv_bind_mat: size mismatch");
     cufsp_status s = mat_coefs(A, 0.0, coefs, E->coefs);
     if (s != CUFSP_SUCCESS) return s;
+    // graphs hold the operator's launch parameters (coefficients included): rebuild them
+    for (auto &g : E->graphs) cudaGraphExecDestroy(g.exec);
+    E->graphs.clear();
     E->A = A;
     E->fn = nullptr;
     return CUFSP_SUCCESS;
@@ -466,6 +571,8 @@ extern "C" cufsp_status cufsp_expv_bind_matvec(cufsp_expv *E, cufsp_matvec_fn fn
     E->fn = fn;
     E->user = user;
     E->A = nullptr;
+    for (auto &g : E->graphs) cudaGraphExecDestroy(g.exec);
+    E->graphs.clear();
     return CUFSP_SUCCESS;
 }
 

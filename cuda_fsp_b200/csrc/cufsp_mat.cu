@@ -29,6 +29,16 @@ cufsp_status mat_apply(cufsp_mat *A, const double *coefs, double alpha, const do
     return sparse_apply(A->sparse, coefs, alpha, d_alpha, d_skip, x, accumulate, y, st, i_begin, i_end);
 }
 
+cufsp_status mat_prepare(cufsp_mat *A, const double *coefs, cudaStream_t st) {
+    return A->kron ? kron_prepare(A->kron, coefs, st) : CUFSP_SUCCESS;
+}
+
+cufsp_status mat_apply_transpose(cufsp_mat *A, const double *coefs, double alpha, const double *d_alpha,
+                                 const int *d_skip, const double *x, double *y, cudaStream_t st) {
+    if (!A->kron) return set_error(CUFSP_ERR_UNSUPPORTED, "transposed generator action needs the KRONECKER format");
+    return kron_apply_transpose(A->kron, coefs, alpha, d_alpha, d_skip, x, y, st);
+}
+
 }  // namespace cufsp
 
 extern "C" cufsp_status cufsp_mat_create(const cufsp_model_desc *desc, cufsp_format format, cufsp_mat **out) {

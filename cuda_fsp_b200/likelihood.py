@@ -149,8 +149,23 @@ class Likelihood:
         self.outside = np.zeros(len(self.times)) if outside is None else np.asarray(outside, np.float64)
         self.p0 = torch.as_tensor(model.p0(), device="cuda")
         self.p = self.p0.clone()
+        self.m, self.kry_tol = m, kry_tol
         self.solver = FSPSolver(self.A, self.p, self.times, fsp_tol, kry_tol, m, coefs=model.coefs(0.0))
         self.fsp_errors: list[float] = []
+
+    def gradient(self, coefs=None, m: int | None = None, tol: float | None = None) -> tuple[float, np.ndarray]:
+        """(log L, d log L / d log c_r) at coefs (default: the model's rates) by the adjoint method
+        (cufsp_likelihood_grad).  Cells outside the box add the constant outside * log(1e-44)."""
+        c = np.ascontiguousarray(np.asarray(self.model.coefs(0.0) if coefs is None else coefs, np.float64))
+        t = np.ascontiguousarray(self.times)
+        lib = self.A._lib
+        ll = C.c_double()
+        g = np.zeros(self.model.nr)
+        _lib.check(lib, lib.cufsp_likelihood_grad(
+            self.A.handle, c.ctypes.data_as(C.POINTER(C.c_double)), len(t), t.ctypes.data_as(C.POINTER(C.c_double)),
+            self.p0.data_ptr(), self.block, self.counts.data_ptr(), int(m or self.m), float(tol or self.kry_tol),
+            C.byref(ll), g.ctypes.data_as(C.POINTER(C.c_double)), _stream(None)), "cufsp_likelihood_grad")
+        return ll.value + float(np.sum(self.outside)) * math.log(1e-44), g
 
     def evaluate(self, coefs=None) -> float:
         if coefs is not None:

@@ -247,6 +247,19 @@ cufsp_status cufsp_solver_reset_time(cufsp_solver *S);
  * (block = 1: no marginalisation).  d_p, d_counts: device, n and n/block doubles.  Synchronous. */
 cufsp_status cufsp_loglik(int64_t n, const double *d_p, int64_t block, const double *d_counts, double *out,
                           cufsp_stream_t stream);
+/* Gradient of the log-likelihood above over several data times by the adjoint method (no counterpart
+ * in the reference; its Likelihood has no gradient):
+ *   log L(c) = sum_i sum_k counts_i[k] log max(1e-44, q_i[k]),  q_i = block sums of exp(times[i] A(c)) p0,
+ *   grad[r] = d log L / d log c_r  (host, n_reactions),  *logL (host).
+ * A: a KRONECKER generator (its transposed action is used); coefs (host, n_reactions) are the rates
+ * c_r of the time-invariant A(c) = sum_r c_r A_r; times (host, n_times, non-decreasing, > 0);
+ * d_p0 (device, n states); d_counts (device, n_times x n / block).  The forward Krylov solve (m, tol
+ * as cufsp_expv_create) keeps p at every step boundary; the backward pass integrates the adjoint with
+ * the transposed generator and accumulates int lambda^T A_r p ds exactly within the two Krylov
+ * subspaces of every step.  Synchronous. */
+cufsp_status cufsp_likelihood_grad(cufsp_mat *A, const double *coefs, int n_times, const double *times,
+                                   const double *d_p0, int64_t block, const double *d_counts, int m, double tol,
+                                   double *logL, double *grad, cufsp_stream_t stream);
 /* generate_data (src/Likelihood.cpp:35-84): Gillespie direct method from x0 (host, n_species
  * ints), an independent trajectory per (time, cell) as single-cell snapshots are, Philox streams
  * seeded by `seed`.  Propensities c_r * prod_s f_{r,s}(x_s) from the model's factor tables

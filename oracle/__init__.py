@@ -286,3 +286,55 @@ def toggle_factor_tables(bounds) -> np.ndarray:
     out = np.empty((6, int(b[0]) + int(b[1]) + 2), np.float64)
     lib().orc_toggle_factor_tables(_p(b), _p(out))
     return out
+
+
+# ---- log-likelihood and its gradient (reference for the adjoint) -------------------------------
+# log L(c) = sum_i sum_k D_i[k] log max(1e-44, q_i[k]), q_i = block sums of exp(t_i A(c)) p0
+# (src/Likelihood.cpp:14-21 over several data times, marginalised over the fastest `block` states).
+
+def _block_sums(p, block):
+    return p.reshape(-1, block).sum(axis=1)
+
+
+def loglik(csr: CSR, coefs, times, p0, counts, block: int = 1) -> float:
+    """log L by scipy's expm_multiply on A(c) (FP64, exact to rounding for these sizes)."""
+    from scipy.sparse.linalg import expm_multiply
+    A = csr.to_scipy(np.asarray(coefs, np.float64)).tocsc()
+    p, t_prev, ll = np.asarray(p0, np.float64).copy(), 0.0, 0.0
+    for i, t in enumerate(times):
+        if t > t_prev:
+            p = expm_multiply((t - t_prev) * A, p)
+        t_prev = t
+        q = _block_sums(p, block)
+        ll += float(np.sum(counts[i] * np.log(np.maximum(1e-44, q))))
+    return ll
+
+
+def loglik_grad_forward(csr: CSR, coefs, times, p0, counts, block: int = 1):
+    """d log L / d log c_r by forward sensitivities: [p; s_r]' = [[A, 0], [A_r, A]] [p; s_r],
+    s_r(0) = 0, so s_r(t) = d p(t) / d c_r; then d log L / d c_r = sum_i g_i^T s_r(t_i) with
+    g_i = M^T (D_i / q_i).  Returns (log L, gradient wrt log c)."""
+    import scipy.sparse as sp
+    from scipy.sparse.linalg import expm_multiply
+    c = np.asarray(coefs, np.float64)
+    n, nr = csr.n, csr.nr
+    A = csr.to_scipy(c)
+    grads = np.zeros(nr)
+    ll = loglik(csr, c, times, p0, counts, block)
+    for r in range(nr):
+        e = np.zeros(nr)
+        e[r] = 1.0
+        Ar = csr.to_scipy(e)
+        Z = sp.csr_matrix((n, n))
+        Aug = sp.bmat([[A, Z], [Ar, A]]).tocsc()
+        y = np.concatenate([np.asarray(p0, np.float64), np.zeros(n)])
+        t_prev = 0.0
+        for i, t in enumerate(times):
+            if t > t_prev:
+                y = expm_multiply((t - t_prev) * Aug, y)
+            t_prev = t
+            p, s = y[:n], y[n:]
+            q = _block_sums(p, block)
+            gq = np.where(q > 1e-44, counts[i] / np.where(q > 1e-44, q, 1.0), 0.0)
+            grads[r] += float(np.dot(np.repeat(gq, block), s))
+    return ll, grads * c
