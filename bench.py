@@ -12,7 +12,11 @@ the full state vector through the C ABI (cufsp_mat_apply, accumulate form).
   roofline  the kernel's achieved GB/s against the measured HBM copy bandwidth
   cpu_baseline  the FP64 host oracle (OpenMP CSR SpMV restating the reference's assembly) timed on
             the host cores on a bounded sample (box 255 x 255 x 63, about 10 s)
-  secondary expmv solves/s on birth_death_2 (32,768 states, t = 10, m = 30, tol 1e-8)
+  secondary [expmv solves/s on birth_death_2 (32,768 states, t = 10, m = 30, tol 1e-8) with the
+             oracle's host solve time beside it;
+             batched expmv solves/s on 256 gene-expression parameter sets (one persistent launch) with
+             the plain single-instance path timed on a sample of the same instances;
+             grad logL grads/s on the 131,072-state gene-expression model (adjoint)]
 
 --impl reference: the reference has no CPU implementation of this path; its CPU restatement (the
 oracle, "port") is timed on the same metric and workload sample with all host threads.
@@ -202,6 +206,87 @@ def expmv_secondary() -> dict:
             "matvecs": st["n_matvec"]}
 
 
+def cpu_expmv_ms() -> float:
+    """The oracle's host Krylov exp(tA)v on birth_death_2 (same workload as the expmv leg)."""
+    import oracle
+    from cuda_fsp_b200 import models
+    m = models.birth_death_2()
+    csr = oracle.assemble_model(m)
+    t0 = time.perf_counter()
+    w, st, rc = oracle.expv(csr, m.coefs(0), 10.0, m.p0(), m=30, tol=1e-8)
+    return (time.perf_counter() - t0) * 1e3
+
+
+def batched_secondary(n_sets: int = 256, sample: int = 4) -> dict:
+    """C4: n_sets parameter sets of the gene-expression model (rates within one decade of nominal,
+    mRNA bounds 63..255) solved to t = 30 in one persistent launch; the plain single-instance Krylov
+    path is timed on `sample` of the same instances and its results compared (1-norm)."""
+    import torch
+    from cuda_fsp_b200 import BatchKrylov, FSPMat, KryExpvFSP, MatrixFormat, models
+    ms = models.gene_batch(n_sets)
+    B = BatchKrylov.from_models(ms, m=30, tol=1e-8)
+    p0 = B.pack([mm.p0() for mm in ms])
+    p = p0.clone()
+    t0 = time.perf_counter()
+    B.solve(30.0, p)  # chooses the launch shape (autotuner) and warms up; untimed
+    tune_s = time.perf_counter() - t0
+    p.copy_(p0)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    stats = B.solve(30.0, p)
+    torch.cuda.synchronize()
+    batch_s = time.perf_counter() - t0
+    out = B.unpack(p)
+    idx = [i * n_sets // sample for i in range(sample)]
+    single_s, errs = 0.0, []
+    for i in idx:
+        mm = ms[i]
+        A = FSPMat.from_model(mm, MatrixFormat.KRONECKER)
+        v = torch.as_tensor(mm.p0(), device="cuda")
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        KryExpvFSP(30.0, A, v, m=30, tol=1e-8, coefs=mm.coefs(0)).solve()
+        torch.cuda.synchronize()
+        single_s += time.perf_counter() - t0
+        errs.append(float(np.abs(v.cpu().numpy() - out[i]).sum()))
+    return {"metric": "batched expmv solves/s", "workload": f"{n_sets} gene-expression parameter sets, "
+            f"{int(B.sizes.sum())} states in total, t = 30, m = 30, tol 1e-8, one persistent launch",
+            "value": round(n_sets / batch_s, 3), "s_per_batch": round(batch_s, 3),
+            "single_instance_solves_per_s": round(len(idx) / single_s, 3),
+            "single_instance_sample": f"{len(idx)} of the same instances through KryExpvFSP",
+            "max_1norm_diff_vs_single": max(errs), "steps_mean": float(np.mean([s_["steps"] for s_ in stats])),
+            "launch": B.describe(), "autotune_and_warmup_s": round(tune_s, 1)}
+
+
+def gradient_secondary(n_grad: int = 2) -> dict:
+    """C5: d log L / d log theta for the 12 rates of the gene-expression model (131,072 states) from
+    1,000 seeded-SSA cells at 8 log-spaced times in [1, 60], (n, c) histograms marginalised over the
+    gene states; timed for n_grad of the parameter sets (each a full forward + adjoint solve)."""
+    import torch
+    from cuda_fsp_b200 import Likelihood, generate_data, histograms, models
+    m = models.gene_expression((1, 1, 1, 127, 127), time_varying=False)
+    times = np.geomspace(1.0, 60.0, 8)
+    snaps = generate_data(m, times, [0, 0, 0, 0, 0], 1000, seed=20261205)
+    counts, outside = histograms(snaps, m.bounds, n_marginal=3)
+    L = Likelihood(m, times, counts, outside=outside, n_marginal=3, kry_tol=1e-8)
+    rng = np.random.default_rng(7)
+    sets = [m.coefs(0) * 10.0 ** rng.uniform(-0.5, 0.5, m.nr) for _ in range(n_grad)]
+    L.gradient(sets[0])  # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for c in sets:
+        L.gradient(c)
+    torch.cuda.synchronize()
+    dt = (time.perf_counter() - t0) / n_grad
+    t0 = time.perf_counter()
+    L.evaluate(sets[0])
+    torch.cuda.synchronize()
+    ev = time.perf_counter() - t0
+    return {"metric": "grad logL grads/s", "workload": "gene_expression 131,072 states, 12 rates, 8 times in [1, 60], "
+            "1,000 SSA cells per time, marginalised over gene states", "value": round(1.0 / dt, 3),
+            "s_per_gradient": round(dt, 3), "s_per_loglik": round(ev, 3), "parameter_sets_timed": n_grad}
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -285,7 +370,12 @@ def run_ours(args):
         e2e_s = t.item()
     e2e_gbs = BYTES_PER_STATE * n / e2e_s / 1e9 * world
 
-    secondary = expmv_secondary() if rank == 0 else None
+    secondary = None
+    if rank == 0:
+        secondary = expmv_secondary()
+        if world == 1:
+            secondary["cpu_oracle_ms_per_solve"] = round(cpu_expmv_ms(), 1)
+        secondary = [secondary, batched_secondary(), gradient_secondary()]
     cpu = cpu_oracle_gbs(max(3, min(args.steps, 20)), 1) if (rank == 0 and world == 1) else None
     peak, peak_kind = measured_peak_hbm()
     if rank == 0:
