@@ -117,3 +117,44 @@ class BatchKrylov:
             self.close()
         except Exception:
             pass
+
+
+def _main(argv=None) -> None:
+    """Solve models.gene_batch(sets, lo..hi mRNA bounds) to t and print the launch shape and totals
+    (used to reproduce the profiles of the batched kernel)."""
+    import argparse
+    import json
+    import time
+
+    import torch
+
+    from . import models
+    ap = argparse.ArgumentParser(prog="python -m cuda_fsp_b200.batch")
+    ap.add_argument("--sets", type=int, default=16)
+    ap.add_argument("--lo", type=int, default=40)
+    ap.add_argument("--hi", type=int, default=60)
+    ap.add_argument("--t", type=float, default=1.0)
+    ap.add_argument("--m", type=int, default=30)
+    ap.add_argument("--cluster", type=int, default=8)
+    ap.add_argument("--threads", type=int, default=256)
+    ap.add_argument("--repeat", type=int, default=2)
+    a = ap.parse_args(argv)
+    ms = models.gene_batch(a.sets, lo=a.lo, hi=a.hi)
+    B = BatchKrylov.from_models(ms, m=a.m, tol=1e-8)
+    if a.cluster > 0:
+        B.set_shape(a.cluster, a.threads)
+    p0 = B.pack([mm.p0() for mm in ms])
+    dt, st = 0.0, []
+    for _ in range(a.repeat):
+        p = p0.clone()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        st = B.solve(a.t, p)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+    print(json.dumps({"launch": B.describe(), "states": int(B.sizes.sum()), "steps": sum(s["steps"] for s in st),
+                      "matvecs": sum(s["matvecs"] for s in st), "s_last_solve": round(dt, 4)}))
+
+
+if __name__ == "__main__":
+    _main()

@@ -21,7 +21,10 @@
 //   I_r += sum_{b'} v_{b'}(x) a_r(x) (uhat_{b'}(x + nu_r) 1{x + nu_r in box} - uhat_{b'}(x))
 // for all reactions at once, with a deterministic grid reduction.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -238,6 +241,15 @@ extern "C" cufsp_status cufsp_likelihood_grad(cufsp_mat *A, const double *coefs,
     // ---- forward pass with checkpoints ----
     CUFSP_CUDA_TRY(cudaMemcpyAsync(p, d_p0, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
     std::vector<std::vector<Checkpoint>> steps(n_times);
+    double *ck_next = nullptr;
+    int ck_left = 0;
+    // optional phase timers (CUFSP_VERBOSE=1)
+    const bool verbose = getenv("CUFSP_VERBOSE") && atoi(getenv("CUFSP_VERBOSE")) != 0;
+    using clk = std::chrono::steady_clock;
+    double t_fwd = 0, t_arn = 0, t_bstep = 0, t_vl = 0, t_kern = 0;
+    int n_sub = 0;
+    auto since = [](clk::time_point a) { return std::chrono::duration<double>(clk::now() - a).count(); };
+    const clk::time_point t_start = clk::now();
     double ll = 0.0, t_prev = 0.0;
     for (int i = 0; i < n_times; ++i) {
         const double dt = times[i] - t_prev;
@@ -249,8 +261,14 @@ extern "C" cufsp_status cufsp_likelihood_grad(cufsp_mat *A, const double *coefs,
             if (s != CUFSP_SUCCESS) return s;
             int reached = 0;
             while (!reached) {
-                double *ck = wk.alloc(n);
-                if (!ck) return set_error(CUFSP_ERR_ALLOC, "cufsp_likelihood_grad: checkpoint allocation failed");
+                if (ck_left == 0) {  // checkpoints are allocated 16 vectors at a time
+                    ck_next = wk.alloc((size_t)n * 16);
+                    if (!ck_next) return set_error(CUFSP_ERR_ALLOC, "cufsp_likelihood_grad: checkpoint allocation failed");
+                    ck_left = 16;
+                }
+                double *ck = ck_next;
+                ck_next += n;
+                --ck_left;
                 CUFSP_CUDA_TRY(cudaMemcpyAsync(ck, p, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
                 s = expv_step_once(ef.E, p, st);
                 if (s != CUFSP_SUCCESS) return s;
@@ -267,6 +285,8 @@ extern "C" cufsp_status cufsp_likelihood_grad(cufsp_mat *A, const double *coefs,
     }
 
     // ---- backward pass ----
+    CUFSP_CUDA_TRY(cudaStreamSynchronize(st));
+    t_fwd = since(t_start);
     CUFSP_CUDA_TRY(cudaMemsetAsync(lam, 0, sizeof(double) * n, st));
     BilinArgs ba;
     std::memset(&ba, 0, sizeof(ba));
@@ -315,9 +335,11 @@ extern "C" cufsp_status cufsp_likelihood_grad(cufsp_mat *A, const double *coefs,
             const double h = ck.tau;
             const double s0 = s_end - h;
             // forward basis on this step from its checkpoint
+            clk::time_point tp = clk::now();
             CUFSP_CUDA_TRY(cudaMemcpyAsync(pf, ck.p, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
             s = expv_arnoldi(ef.E, pf, st);
             if (s != CUFSP_SUCCESS) return s;
+            t_arn += since(tp);
             const KrylovStep F = expv_last(ef.E);
             // lambda backward over [s0, s_end] in adaptive sub-steps
             CUFSP_CUDA_TRY(cudaStreamSynchronize(st));
@@ -327,14 +349,18 @@ extern "C" cufsp_status cufsp_likelihood_grad(cufsp_mat *A, const double *coefs,
             double b_end = s_end;
             int reached = h <= 0.0;
             while (!reached) {
+                tp = clk::now();
                 CUFSP_CUDA_TRY(cudaMemcpyAsync(lam_b, lam, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
                 s = expv_step_once(eb.E, lam, st);
                 if (s != CUFSP_SUCCESS) return s;
+                t_bstep += since(tp);
+                ++n_sub;
                 const KrylovStep B = expv_last(eb.E);
                 cufsp_expv_final_time_reached(eb.E, &reached);
                 const double tau = B.tau;
                 const double a0 = b_end - tau;
                 if (F.beta > 0.0 && B.beta > 0.0 && tau > 0.0) {
+                    tp = clk::now();
                     // W = upper-right mb_b x mb_f block of exp(tau [[G, z_b y_a^T], [0, H^T]])
                     s = dense_output(F.mb, F.H, a0 - s0, F.beta, ya);
                     if (s != CUFSP_SUCCESS) return s;
@@ -354,6 +380,8 @@ extern "C" cufsp_status cufsp_likelihood_grad(cufsp_mat *A, const double *coefs,
                     for (int aa = 0; aa < mbb; ++aa)
                         for (int bb = 0; bb < mbf; ++bb)
                             coefm[(size_t)aa * mbf + bb] = Fb[aa + (size_t)(mbb + bb) * K] * B.rho[aa];
+                    t_vl += since(tp);
+                    tp = clk::now();
                     CUFSP_CUDA_TRY(cudaMemcpyAsync(d_coef, coefm.data(), sizeof(double) * coefm.size(),
                                                    cudaMemcpyHostToDevice, st));
                     CombManyArgs ca;
@@ -374,6 +402,7 @@ extern "C" cufsp_status cufsp_likelihood_grad(cufsp_mat *A, const double *coefs,
                     k_adj_bilinear<<<red_grid, kRedThreads, 0, st>>>(ba);
                     CUFSP_CUDA_TRY(cudaGetLastError());
                     CUFSP_CUDA_TRY(cudaStreamSynchronize(st));  // d_coef / uh are reused by the next sub-step
+                    t_kern += since(tp);
                 }
                 b_end = a0;
             }
@@ -384,6 +413,14 @@ extern "C" cufsp_status cufsp_likelihood_grad(cufsp_mat *A, const double *coefs,
     CUFSP_CUDA_TRY(cudaMemcpyAsync(I.data(), d_I, sizeof(double) * nr, cudaMemcpyDeviceToHost, st));
     CUFSP_CUDA_TRY(cudaStreamSynchronize(st));
     (void)d_ll;
+    if (verbose) {
+        size_t nsteps = 0;
+        for (auto &v : steps) nsteps += v.size();
+        fprintf(stderr,
+                "cufsp_likelihood_grad: %zu forward steps, %d backward sub-steps; forward %.3f s, basis rebuild "
+                "%.3f s, backward steps %.3f s, Van Loan %.3f s, step integrals %.3f s, total %.3f s\n",
+                nsteps, n_sub, t_fwd, t_arn, t_bstep, t_vl, t_kern, since(t_start));
+    }
     *logL = ll;
     for (int r = 0; r < nr; ++r) grad[r] = c[r] * I[r];  // d log L / d log c_r
     return CUFSP_SUCCESS;

@@ -18,15 +18,14 @@ namespace cufsp {
 
 namespace {
 
-void matmul(int k, const double *A, const double *B, double *C) {
-    // C = A * B, column-major; loop order j-l-i keeps the inner loop unit-stride.
+void matmul(int k, const double *__restrict A, const double *__restrict B, double *__restrict C) {
+    // C = A * B, column-major; loop order j-l-i keeps the inner loop unit-stride (vectorisable).
     for (int j = 0; j < k; ++j) {
-        double *cj = C + (size_t)j * k;
+        double *__restrict cj = C + (size_t)j * k;
         for (int i = 0; i < k; ++i) cj[i] = 0.0;
         for (int l = 0; l < k; ++l) {
             const double b = B[l + (size_t)j * k];
-            if (b == 0.0) continue;
-            const double *al = A + (size_t)l * k;
+            const double *__restrict al = A + (size_t)l * k;
             for (int i = 0; i < k; ++i) cj[i] += al[i] * b;
         }
     }
