@@ -146,6 +146,8 @@ SIGNATURES = {
     "cufsp_solver_reset_time": [_P],
     "cufsp_loglik": [C.c_int64, _P, C.c_int64, _P, _DP, _P],
     "cufsp_likelihood_grad": [_P, _DP, C.c_int, _DP, _P, C.c_int64, _P, C.c_int, C.c_double, _DP, _DP, _P],
+    "cufsp_likelihood_grad_batched": [C.POINTER(ModelDesc), C.c_int, _DP, C.c_int, _DP, _P, C.c_int64, _P, C.c_int,
+                                      C.c_double, C.c_int, _DP, _DP],
     "cufsp_ssa": [C.POINTER(ModelDesc), _DP, _IP, _DP, C.c_int, C.c_int, C.c_ulonglong, C.c_int64, _P, _P],
     "cufsp_vec_sum": [C.c_int64, _P, _DP, _P],
     "cufsp_batch_create": [C.POINTER(BatchDesc), C.c_int, C.c_double, C.c_int, C.c_int, C.POINTER(_P)],

@@ -21,7 +21,10 @@
 //   I_r += sum_{b'} v_{b'}(x) a_r(x) (uhat_{b'}(x + nu_r) 1{x + nu_r in box} - uhat_{b'}(x))
 // for all reactions at once, with a deterministic grid reduction.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
+#include <string>
+#include <thread>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -47,6 +50,11 @@ __global__ void k_loglik_grad_vec(int64_t n, const double *__restrict__ p, int64
         const double v = (q > 1e-44 && d != 0.0) ? d / q : 0.0;
         for (int64_t j = 0; j < block; ++j) g[k * block + j] = v;
     }
+}
+
+__global__ void k_scale_vec(int64_t n, double a, double *__restrict__ x) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        x[i] *= a;
 }
 
 __global__ void k_axpy(int64_t n, double a, const double *__restrict__ x, double *__restrict__ y) {
@@ -341,8 +349,17 @@ extern "C" cufsp_status cufsp_likelihood_grad(cufsp_mat *A, const double *coefs,
             if (s != CUFSP_SUCCESS) return s;
             t_arn += since(tp);
             const KrylovStep F = expv_last(ef.E);
-            // lambda backward over [s0, s_end] in adaptive sub-steps
+            // lambda backward over [s0, s_end] in adaptive sub-steps.  Expokit's error test is
+            // absolute while |lambda| grows with the counts (g = D / q), so lambda is scaled to unit
+            // norm for the solve and the step integrals are scaled back.
+            s = launch_nrm2(n, lam, d_ll, rs, st);
+            if (s != CUFSP_SUCCESS) return s;
+            double lnorm = 0.0;
+            CUFSP_CUDA_TRY(cudaMemcpyAsync(&lnorm, d_ll, sizeof(double), cudaMemcpyDeviceToHost, st));
             CUFSP_CUDA_TRY(cudaStreamSynchronize(st));
+            const double lscale = (lnorm > 0.0 && std::isfinite(lnorm)) ? lnorm : 1.0;
+            k_scale_vec<<<vgrid, 256, 0, st>>>(n, 1.0 / lscale, lam);
+            CUFSP_CUDA_TRY(cudaGetLastError());
             s = cufsp_expv_set_final_time(eb.E, h);
             if (s == CUFSP_SUCCESS) s = cufsp_expv_reset_time(eb.E);
             if (s != CUFSP_SUCCESS) return s;
@@ -379,7 +396,7 @@ extern "C" cufsp_status cufsp_likelihood_grad(cufsp_mat *A, const double *coefs,
                     coefm.assign((size_t)mbb * mbf, 0.0);
                     for (int aa = 0; aa < mbb; ++aa)
                         for (int bb = 0; bb < mbf; ++bb)
-                            coefm[(size_t)aa * mbf + bb] = Fb[aa + (size_t)(mbb + bb) * K] * B.rho[aa];
+                            coefm[(size_t)aa * mbf + bb] = lscale * Fb[aa + (size_t)(mbb + bb) * K] * B.rho[aa];
                     t_vl += since(tp);
                     tp = clk::now();
                     CUFSP_CUDA_TRY(cudaMemcpyAsync(d_coef, coefm.data(), sizeof(double) * coefm.size(),
@@ -406,6 +423,8 @@ extern "C" cufsp_status cufsp_likelihood_grad(cufsp_mat *A, const double *coefs,
                 }
                 b_end = a0;
             }
+            k_scale_vec<<<vgrid, 256, 0, st>>>(n, lscale, lam);
+            CUFSP_CUDA_TRY(cudaGetLastError());
             s_end = s0;
         }
     }
@@ -423,5 +442,52 @@ extern "C" cufsp_status cufsp_likelihood_grad(cufsp_mat *A, const double *coefs,
     }
     *logL = ll;
     for (int r = 0; r < nr; ++r) grad[r] = c[r] * I[r];  // d log L / d log c_r
+    return CUFSP_SUCCESS;
+}
+
+// Many parameter sets: `workers` host threads, each with its own generator (the plane kernel keeps
+// coefficient-dependent tables per generator), stream and Krylov workspaces, take sets from a shared
+// counter; their solves overlap on the GPU.
+extern "C" cufsp_status cufsp_likelihood_grad_batched(const cufsp_model_desc *desc, int n_sets, const double *coefs,
+                                                      int n_times, const double *times, const double *d_p0,
+                                                      int64_t block, const double *d_counts, int m, double tol,
+                                                      int workers, double *logL, double *grad) {
+    clear_error();
+    if (!desc || !coefs || !logL || !grad || n_sets < 1)
+        return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_likelihood_grad_batched: bad argument");
+    const int nr = desc->n_reactions;
+    workers = std::max(1, std::min(std::min(workers, n_sets), 32));
+    int dev = 0;
+    CUFSP_CUDA_TRY(cudaGetDevice(&dev));
+    std::atomic<int> next(0);
+    std::vector<cufsp_status> status(workers, CUFSP_SUCCESS);
+    std::vector<std::string> msg(workers);
+    auto work = [&](int w) {
+        cudaSetDevice(dev);
+        cufsp_mat *A = nullptr;
+        cudaStream_t st = nullptr;
+        cufsp_status s = cufsp_mat_create(desc, CUFSP_FORMAT_KRONECKER, &A);
+        if (s == CUFSP_SUCCESS && cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess)
+            s = set_error(CUFSP_ERR_CUDA, "stream creation failed");
+        while (s == CUFSP_SUCCESS) {
+            const int i = next.fetch_add(1);
+            if (i >= n_sets) break;
+            s = cufsp_likelihood_grad(A, coefs + (size_t)i * nr, n_times, times, d_p0, block, d_counts, m, tol,
+                                      logL + i, grad + (size_t)i * nr, (cufsp_stream_t)st);
+        }
+        if (s != CUFSP_SUCCESS) {
+            status[w] = s;
+            msg[w] = cufsp_last_error();
+            next.store(n_sets);  // the other workers stop at their next set
+        }
+        if (st) cudaStreamDestroy(st);
+        cufsp_mat_destroy(A);
+    };
+    std::vector<std::thread> pool;
+    for (int w = 1; w < workers; ++w) pool.emplace_back(work, w);
+    work(0);
+    for (auto &t : pool) t.join();
+    for (int w = 0; w < workers; ++w)
+        if (status[w] != CUFSP_SUCCESS) return set_error(status[w], "cufsp_likelihood_grad_batched: " + msg[w]);
     return CUFSP_SUCCESS;
 }

@@ -83,6 +83,22 @@ class FSPSolver:
             pass
 
 
+def _model_desc(model):
+    """cufsp_model_desc of a models.CMEModel (factor tables, no time coefficients); returns the
+    descriptor and the arrays it points into (keep them alive while the descriptor is used)."""
+    b = np.ascontiguousarray(np.asarray(model.bounds, np.int32))
+    sv, sc, sr = model.stoich_csr()
+    tab = np.ascontiguousarray(model.tables, np.float64)
+    d = ModelDesc()
+    d.n_species, d.n_reactions = model.ns, model.nr
+    d.fsp_bounds = b.ctypes.data_as(C.POINTER(C.c_int))
+    d.stoich_vals = sv.ctypes.data_as(C.POINTER(C.c_int))
+    d.stoich_colidxs = sc.ctypes.data_as(C.POINTER(C.c_int))
+    d.stoich_rowptrs = sr.ctypes.data_as(C.POINTER(C.c_int))
+    d.factor_tables = tab.ctypes.data_as(C.POINTER(C.c_double))
+    return d, (b, sv, sc, sr, tab)
+
+
 def generate_data(model, times, x0, n_cells: int, seed: int = 20261203, coefs=None, max_events: int = 10**8,
                   lib=None) -> np.ndarray:
     """Seeded SSA snapshots: int32 array [n_times, n_cells, n_species], an independent trajectory
@@ -166,6 +182,23 @@ class Likelihood:
             self.p0.data_ptr(), self.block, self.counts.data_ptr(), int(m or self.m), float(tol or self.kry_tol),
             C.byref(ll), g.ctypes.data_as(C.POINTER(C.c_double)), _stream(None)), "cufsp_likelihood_grad")
         return ll.value + float(np.sum(self.outside)) * math.log(1e-44), g
+
+    def gradient_batched(self, coef_sets, workers: int = 8, m: int | None = None,
+                         tol: float | None = None) -> tuple[np.ndarray, np.ndarray]:
+        """(log L [n_sets], d log L / d log c [n_sets, n_reactions]) for many parameter sets at once
+        (cufsp_likelihood_grad_batched: `workers` concurrent adjoint solves on the GPU)."""
+        c = np.ascontiguousarray(np.asarray(coef_sets, np.float64).reshape(-1, self.model.nr))
+        ns = c.shape[0]
+        t = np.ascontiguousarray(self.times)
+        lib = self.A._lib
+        d, _keep = _model_desc(self.model)
+        ll = np.zeros(ns)
+        g = np.zeros((ns, self.model.nr))
+        dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))  # noqa: E731
+        _lib.check(lib, lib.cufsp_likelihood_grad_batched(
+            C.byref(d), ns, dp(c), len(t), dp(t), self.p0.data_ptr(), self.block, self.counts.data_ptr(),
+            int(m or self.m), float(tol or self.kry_tol), int(workers), dp(ll), dp(g)), "cufsp_likelihood_grad_batched")
+        return ll + float(np.sum(self.outside)) * math.log(1e-44), g
 
     def evaluate(self, coefs=None) -> float:
         if coefs is not None:

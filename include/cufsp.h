@@ -260,6 +260,14 @@ cufsp_status cufsp_loglik(int64_t n, const double *d_p, int64_t block, const dou
 cufsp_status cufsp_likelihood_grad(cufsp_mat *A, const double *coefs, int n_times, const double *times,
                                    const double *d_p0, int64_t block, const double *d_counts, int m, double tol,
                                    double *logL, double *grad, cufsp_stream_t stream);
+/* The same gradient for n_sets parameter sets (coefs: host [n_sets][n_reactions]; logL: host [n_sets];
+ * grad: host [n_sets][n_reactions]) sharing times, p0 and counts.  `workers` host threads, each with
+ * its own KRONECKER generator built from desc, stream and workspaces, overlap their solves on the
+ * GPU.  No counterpart in the reference.  Synchronous. */
+cufsp_status cufsp_likelihood_grad_batched(const cufsp_model_desc *desc, int n_sets, const double *coefs,
+                                           int n_times, const double *times, const double *d_p0, int64_t block,
+                                           const double *d_counts, int m, double tol, int workers, double *logL,
+                                           double *grad);
 /* generate_data (src/Likelihood.cpp:35-84): Gillespie direct method from x0 (host, n_species
  * ints), an independent trajectory per (time, cell) as single-cell snapshots are, Philox streams
  * seeded by `seed`.  Propensities c_r * prod_s f_{r,s}(x_s) from the model's factor tables

@@ -94,3 +94,18 @@ def test_adjoint_rejects_bad_requests(cuda):
     with pytest.raises(CufspError) as ei:
         L.gradient()
     assert ei.value.name == "CUFSP_ERR_UNSUPPORTED"
+
+
+def test_batched_gradients_equal_single_gradients(cuda):
+    """cufsp_likelihood_grad_batched (concurrent workers) gives each set's single-call result."""
+    m = models.gene_expression((1, 1, 1, 15, 15), time_varying=False)
+    times = np.array([1.0, 4.0, 12.0])
+    counts = synthetic_counts(m, times, 8, 300, seed=5)
+    L = Likelihood(m, times, counts, n_marginal=3, kry_tol=1e-10)
+    rng = np.random.default_rng(6)
+    sets = np.stack([m.coefs(0) * np.exp(rng.uniform(-0.5, 0.5, m.nr)) for _ in range(6)])
+    ll, g = L.gradient_batched(sets, workers=3)
+    for i in range(6):
+        lli, gi = L.gradient(sets[i])
+        assert abs(ll[i] - lli) <= 1e-12 * abs(lli)
+        assert np.max(np.abs(g[i] - gi)) <= 1e-12 * np.max(np.abs(gi))
