@@ -44,7 +44,10 @@ struct BatchKernel {
 
 std::mutex g_batch_mu;
 std::map<std::string, std::shared_ptr<BatchKernel>> g_batch_cache;
-std::map<std::string, std::pair<int, int>> g_tune_cache;  // key -> (cluster CTAs, threads)
+struct Shape {
+    int cluster, threads, minb;
+};
+std::map<std::string, Shape> g_tune_cache;  // key -> launch shape
 
 int env_int(const char *name, int dflt) {
     const char *v = getenv(name);
@@ -115,12 +118,11 @@ std::string cache_path() {
     return std::string(home ? home : "/tmp") + "/.cache/cufsp_batch_autotune.txt";
 }
 
-bool cache_lookup(const std::string &key, int &c, int &t) {
+bool cache_lookup(const std::string &key, Shape &sh) {
     std::lock_guard<std::mutex> lock(g_batch_mu);
     auto it = g_tune_cache.find(key);
     if (it != g_tune_cache.end()) {
-        c = it->second.first;
-        t = it->second.second;
+        sh = it->second;
         return true;
     }
     std::ifstream f(cache_path());
@@ -128,25 +130,25 @@ bool cache_lookup(const std::string &key, int &c, int &t) {
     while (std::getline(f, line)) {
         std::istringstream ls(line);
         std::string k;
-        int cc = 0, tt = 0;
-        if (ls >> k >> cc >> tt && k == key && cc > 0 && tt > 0) {
-            g_tune_cache[key] = {cc, tt};
-            c = cc;
-            t = tt;
+        Shape s2{0, 0, 0};
+        if (ls >> k >> s2.cluster >> s2.threads >> s2.minb && k == key && s2.cluster > 0 && s2.threads > 0 &&
+            s2.minb > 0) {
+            g_tune_cache[key] = s2;
+            sh = s2;
             return true;
         }
     }
     return false;
 }
 
-void cache_store(const std::string &key, int c, int t, double ms) {
+void cache_store(const std::string &key, const Shape &sh, double ms) {
     std::lock_guard<std::mutex> lock(g_batch_mu);
-    g_tune_cache[key] = {c, t};
+    g_tune_cache[key] = sh;
     const std::string path = cache_path();
     const size_t slash = path.rfind('/');
     if (slash != std::string::npos && slash > 0) mkdir(path.substr(0, slash).c_str(), 0755);  // one level
     std::ofstream f(path, std::ios::app);
-    if (f) f << key << " " << c << " " << t << " " << ms << "\n";
+    if (f) f << key << " " << sh.cluster << " " << sh.threads << " " << sh.minb << " " << ms << "\n";
 }
 
 }  // namespace
@@ -175,7 +177,7 @@ struct cufsp_batch_s {
     size_t work_doubles = 0;
     double *d_scratch = nullptr;           // autotuner trial vectors
     // chosen launch shape
-    int cluster = 0, threads = 0;
+    int cluster = 0, threads = 0, minb = 1;
     std::shared_ptr<BatchKernel> kern;
     int n_clusters = 0;
     double tuned_ms = 0.0;
@@ -190,9 +192,10 @@ struct cufsp_batch_s {
 
 namespace {
 
-std::string shape_source(const cufsp_batch *B, int threads) {
+// Launch shape: CTAs per cluster, threads per CTA, CTAs per SM promised to the compiler (register cap).
+std::string shape_source(const cufsp_batch *B, int threads, int minb) {
     std::ostringstream s;
-    s << "#define CUFSP_BATCH_THREADS " << threads << "\n" << B->pattern;
+    s << "#define CUFSP_BATCH_THREADS " << threads << "\n#define CUFSP_BATCH_MINB " << minb << "\n" << B->pattern;
     return s.str() + kBatchSource;
 }
 
@@ -264,6 +267,14 @@ cufsp_status launch(cufsp_batch *B, const BatchKernel &k, int cluster, int threa
     return CUFSP_SUCCESS;
 }
 
+std::string describe_shape(const cufsp_batch *B) {
+    std::ostringstream d;
+    d << "batched Krylov (NVRTC, sm_100a, one persistent launch): " << B->n_inst << " instances, m=" << B->m
+      << (B->iop ? " IOP" : "") << ", " << B->n_clusters << " clusters x " << B->cluster << " CTAs x " << B->threads
+      << " threads (" << B->minb << " CTA/SM bound), smem " << B->kern->smem << " B/CTA";
+    return d.str();
+}
+
 std::string tune_key(const cufsp_batch *B) {
     int dev = 0;
     cudaGetDevice(&dev);
@@ -283,31 +294,34 @@ std::string tune_key(const cufsp_batch *B) {
 // vectors) and keep the fastest.
 cufsp_status autotune(cufsp_batch *B, double t_final, const double *p, cudaStream_t st) {
     const std::string key = tune_key(B);
-    int c = env_int("CUFSP_BATCH_CLUSTER", 0), t = env_int("CUFSP_BATCH_THREADS", 0);
+    Shape sh{env_int("CUFSP_BATCH_CLUSTER", 0), env_int("CUFSP_BATCH_THREADS", 0), env_int("CUFSP_BATCH_MINB", 1)};
     std::string why;
-    if (c > 0 && t > 0) {
-        B->cluster = c;
-        B->threads = t;
-    } else if (cache_lookup(key, c, t)) {
-        B->cluster = c;
-        B->threads = t;
+    if (sh.cluster > 0 && sh.threads > 0) {
+        B->cluster = sh.cluster;
+        B->threads = sh.threads;
+        B->minb = std::max(1, sh.minb);
+    } else if (cache_lookup(key, sh)) {
+        B->cluster = sh.cluster;
+        B->threads = sh.threads;
+        B->minb = sh.minb;
     } else {
-        const int cands[][2] = {{4, 256}, {8, 256}, {16, 256}, {8, 512}, {16, 512}};
+        const Shape cands[] = {{8, 256, 1}, {16, 256, 1}, {8, 512, 1}, {16, 512, 1}, {8, 256, 2}, {16, 256, 2}};
         const int64_t total = B->offsets.back();
         if (!B->d_scratch) CUFSP_CUDA_TRY(cudaMalloc(&B->d_scratch, sizeof(double) * (size_t)total));
         double best = 1e300;
         cudaEvent_t e0, e1;
         CUFSP_CUDA_TRY(cudaEventCreate(&e0));
         CUFSP_CUDA_TRY(cudaEventCreate(&e1));
-        for (auto &cd : cands) {
-            auto k = batch_kernel(shape_source(B, cd[1]), why);
+        for (const Shape &cd : cands) {
+            auto k = batch_kernel(shape_source(B, cd.threads, cd.minb), why);
             if (!k) continue;
-            const int ncl = clusters_for(B, *k, cd[0], cd[1]);
+            const int ncl = clusters_for(B, *k, cd.cluster, cd.threads);
             if (ncl < 1) continue;
             if (ensure_work(B, ncl) != CUFSP_SUCCESS) continue;
             CUFSP_CUDA_TRY(cudaMemcpyAsync(B->d_scratch, p, sizeof(double) * (size_t)total, cudaMemcpyDeviceToDevice, st));
             CUFSP_CUDA_TRY(cudaEventRecord(e0, st));
-            cufsp_status s = launch(B, *k, cd[0], cd[1], ncl, t_final, B->d_scratch, B->d_order_sample, B->n_sample, st);
+            cufsp_status s =
+                launch(B, *k, cd.cluster, cd.threads, ncl, t_final, B->d_scratch, B->d_order_sample, B->n_sample, st);
             CUFSP_CUDA_TRY(cudaEventRecord(e1, st));
             if (s != CUFSP_SUCCESS || cudaStreamSynchronize(st) != cudaSuccess) {
                 cudaGetLastError();
@@ -317,28 +331,25 @@ cufsp_status autotune(cufsp_batch *B, double t_final, const double *p, cudaStrea
             cudaEventElapsedTime(&ms, e0, e1);
             if (ms < best) {
                 best = ms;
-                B->cluster = cd[0];
-                B->threads = cd[1];
+                B->cluster = cd.cluster;
+                B->threads = cd.threads;
+                B->minb = cd.minb;
             }
         }
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         if (B->cluster == 0) return set_error(CUFSP_ERR_CUDA, "batched solver: no launch shape fits this device: " + why);
         B->tuned_ms = best;
-        cache_store(key, B->cluster, B->threads, best);
+        cache_store(key, Shape{B->cluster, B->threads, B->minb}, best);
     }
-    B->kern = batch_kernel(shape_source(B, B->threads), why);
+    B->kern = batch_kernel(shape_source(B, B->threads, B->minb), why);
     if (!B->kern) return set_error(CUFSP_ERR_CUDA, "batched solver: " + why);
     B->n_clusters = clusters_for(B, *B->kern, B->cluster, B->threads);
     if (B->n_clusters < 1) return set_error(CUFSP_ERR_UNSUPPORTED, "batched solver: launch shape does not fit");
     cufsp_status s = ensure_work(B, B->n_clusters);
     if (s != CUFSP_SUCCESS) return s;
     B->tuned = true;
-    std::ostringstream d;
-    d << "batched Krylov (NVRTC, sm_100a, one persistent launch): " << B->n_inst << " instances, m=" << B->m
-      << (B->iop ? " IOP" : "") << ", " << B->n_clusters << " clusters x " << B->cluster << " CTAs x " << B->threads
-      << " threads, smem " << B->kern->smem << " B/CTA";
-    B->describe = d.str();
+    B->describe = describe_shape(B);
     return CUFSP_SUCCESS;
 }
 
@@ -472,7 +483,7 @@ extern "C" cufsp_status cufsp_batch_create(const cufsp_batch_desc *d, int m, dou
     }
     // compile the default shape now so that a bad network fails at create
     std::string why;
-    if (!batch_kernel(shape_source(B.get(), 256), why)) {
+    if (!batch_kernel(shape_source(B.get(), 256, 1), why)) {
         cufsp_batch_destroy(B.release());
         return set_error(CUFSP_ERR_CUDA, "cufsp_batch_create: " + why);
     }
@@ -532,8 +543,9 @@ extern "C" cufsp_status cufsp_batch_set_shape(cufsp_batch *B, int cluster_ctas, 
     } else {
         if (cluster_ctas < 1 || cluster_ctas > 16 || (threads != 128 && threads != 256 && threads != 512))
             return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_batch_set_shape: cluster 1..16, threads 128/256/512");
+        const int minb = std::max(1, env_int("CUFSP_BATCH_MINB", 1));
         std::string why;
-        auto k = batch_kernel(shape_source(B, threads), why);
+        auto k = batch_kernel(shape_source(B, threads, minb), why);
         if (!k) return set_error(CUFSP_ERR_CUDA, "cufsp_batch_set_shape: " + why);
         const int ncl = clusters_for(B, *k, cluster_ctas, threads);
         if (ncl < 1) return set_error(CUFSP_ERR_UNSUPPORTED, "cufsp_batch_set_shape: shape does not fit the device");
@@ -541,14 +553,11 @@ extern "C" cufsp_status cufsp_batch_set_shape(cufsp_batch *B, int cluster_ctas, 
         if (s != CUFSP_SUCCESS) return s;
         B->cluster = cluster_ctas;
         B->threads = threads;
+        B->minb = minb;
         B->kern = k;
         B->n_clusters = ncl;
         B->tuned = true;
-        std::ostringstream d;
-        d << "batched Krylov (NVRTC, sm_100a, one persistent launch): " << B->n_inst << " instances, m=" << B->m
-          << (B->iop ? " IOP" : "") << ", " << ncl << " clusters x " << cluster_ctas << " CTAs x " << threads
-          << " threads, smem " << k->smem << " B/CTA";
-        B->describe = d.str();
+        B->describe = describe_shape(B);
     }
     if (B->gexec) {
         cudaGraphExecDestroy(B->gexec);

@@ -601,7 +601,8 @@ __device__ void solve_instance(const CufspBatchArgs &a, cg::cluster_group &cl, S
 // Dynamic shared memory the kernel needs (read by the host after loading).
 extern "C" __device__ const int cufsp_batch_smem_bytes = (int)sizeof(cufsp_batch::Shared);
 
-extern "C" __global__ void __launch_bounds__(CUFSP_BATCH_THREADS, 1) cufsp_batch_expv(const CufspBatchArgs a) {
+extern "C" __global__ void __launch_bounds__(CUFSP_BATCH_THREADS, CUFSP_BATCH_MINB)
+    cufsp_batch_expv(const CufspBatchArgs a) {
     using namespace cufsp_batch;
     extern __shared__ __align__(16) unsigned char dsm[];
     Shared &s = *reinterpret_cast<Shared *>(dsm);
