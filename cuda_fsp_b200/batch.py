@@ -158,3 +158,52 @@ def _main(argv=None) -> None:
 
 if __name__ == "__main__":
     _main()
+
+
+# ---- several GPUs: one rank per GPU, parameter sets partitioned, one final gather --------------
+
+def partition_instances(sizes, world: int) -> list[list[int]]:
+    """Split instance indices over `world` ranks so that the ranks' total state counts are as even as
+    a largest-first greedy assignment makes them (the solve time of an instance grows with its size).
+    Deterministic: every rank computes the same partition."""
+    sizes = np.asarray(sizes, np.int64)
+    load = np.zeros(world, np.int64)
+    parts: list[list[int]] = [[] for _ in range(world)]
+    for i in sorted(range(len(sizes)), key=lambda k: (-int(sizes[k]), k)):
+        r = int(np.argmin(load))
+        parts[r].append(i)
+        load[r] += sizes[i]
+    return [sorted(p) for p in parts]
+
+
+def solve_sharded(models_, t_final: float, rank: int, world: int, m: int = 30, tol: float = 1e-8,
+                  solver=None, group=None) -> list[dict]:
+    """Solve this rank's share of the instances (exp(t_final A_i) p_i(0) from each model's p0) and
+    gather every instance's summary (final mass, steps, status) on all ranks -- the only collective.
+    `solver(models, t)` -> list of (vector, stat) may replace the GPU batch (host tests)."""
+    import torch.distributed as dist
+
+    parts = partition_instances([mm.n_states for mm in models_], world)
+    mine = parts[rank]
+    local: list[tuple[int, dict]] = []
+    if mine:
+        sub = [models_[i] for i in mine]
+        if solver is None:
+            B = BatchKrylov.from_models(sub, m=m, tol=tol)
+            p = B.pack([mm.p0() for mm in sub])
+            stats = B.solve(t_final, p)
+            vecs = B.unpack(p)
+        else:
+            vecs, stats = zip(*solver(sub, t_final))
+        for i, v, st in zip(mine, vecs, stats):
+            local.append((i, {"mass": float(np.sum(v)), "steps": int(st["steps"]), "status": int(st["status"])}))
+    if world == 1:
+        gathered = [local]
+    else:
+        gathered = [None] * world
+        dist.all_gather_object(gathered, local, group=group)
+    out: list[dict] = [{} for _ in models_]
+    for part in gathered:
+        for i, summary in part:
+            out[i] = summary
+    return out
