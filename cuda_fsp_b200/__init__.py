@@ -8,8 +8,8 @@ from . import models
 from ._lib import CufspError
 from .batch import BatchKrylov
 from .fsp import FSPMat, KryExpvFSP, MatrixFormat, expm, get_states, num_states
-from .likelihood import FSPSolver, Likelihood, generate_data, histograms
+from .likelihood import AdaptiveFSP, FSPSolver, Likelihood, generate_data, histograms
 from .ode import BDFIntegrator
 
 __all__ = ["models", "CufspError", "BatchKrylov", "FSPMat", "KryExpvFSP", "MatrixFormat", "expm", "get_states", "num_states",
-           "FSPSolver", "Likelihood", "generate_data", "histograms", "BDFIntegrator"]
+           "FSPSolver", "AdaptiveFSP", "Likelihood", "generate_data", "histograms", "BDFIntegrator"]

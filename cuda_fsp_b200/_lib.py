@@ -94,6 +94,16 @@ class BatchStat(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class AdaptiveStatus(C.Structure):
+    _fields_ = [("time_index", C.c_int), ("t", C.c_double), ("fsp_error", C.c_double), ("fsp_tol_exceeded", C.c_int),
+                ("expansions", C.c_int), ("n_states", C.c_int64), ("bounds", C.c_int * 16)]
+
+    def as_dict(self) -> dict:
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "bounds"}
+        d["bounds"] = list(self.bounds)
+        return d
+
+
 _P = C.c_void_p
 _I64P = C.POINTER(C.c_int64)
 _IP = C.POINTER(C.c_int)
@@ -150,6 +160,13 @@ SIGNATURES = {
                                       C.c_double, C.c_int, _DP, _DP],
     "cufsp_ssa": [C.POINTER(ModelDesc), _DP, _IP, _DP, C.c_int, C.c_int, C.c_ulonglong, C.c_int64, _P, _P],
     "cufsp_vec_sum": [C.c_int64, _P, _DP, _P],
+    "cufsp_vec_copy": [C.c_int64, _P, _P, _P],
+    "cufsp_adaptive_create": [C.POINTER(ModelDesc), _IP, C.c_double, C.c_double, _DP, _DP, C.c_int, C.c_double,
+                              C.c_int, C.POINTER(_P)],
+    "cufsp_adaptive_destroy": [_P],
+    "cufsp_adaptive_set_initial": [_P, _P, _P],
+    "cufsp_adaptive_next_time": [_P, _P, C.POINTER(AdaptiveStatus)],
+    "cufsp_adaptive_solution": [_P, C.POINTER(C.c_void_p), _IP, _I64P],
     "cufsp_batch_create": [C.POINTER(BatchDesc), C.c_int, C.c_double, C.c_int, C.c_int, C.POINTER(_P)],
     "cufsp_batch_destroy": [_P],
     "cufsp_batch_layout": [_P, _I64P],

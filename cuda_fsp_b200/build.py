@@ -28,7 +28,7 @@ NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-rdc=true", "-Xcompiler"
                      "-I" + str(ROOT / "include"), "--expt-relaxed-constexpr", "--extended-lambda"]
 SOURCES = ["cufsp_common.cu", "cufsp_kron.cu", "cufsp_kron_plane.cu", "cufsp_kron_march.cu", "cufsp_sparse.cu", "cufsp_mat.cu",
            "cufsp_krylov.cu", "cufsp_expm.cpp", "cufsp_noalloc.cu", "cufsp_stats.cu", "cufsp_solver.cu",
-           "cufsp_vec.cu", "cufsp_bdf.cu", "cufsp_batch.cu", "cufsp_adjoint.cu"]
+           "cufsp_vec.cu", "cufsp_bdf.cu", "cufsp_batch.cu", "cufsp_adjoint.cu", "cufsp_adaptive.cu"]
 HEADERS = ["cufsp_internal.h", "cufsp_reduce.cuh", "cufsp_march.h", "cufsp_vec.h", "cufsp_plane.cuh", "cufsp_batch.cuh"]
 # Kernel sources compiled at run time by NVRTC are embedded in the library as string literals.
 RTC_SOURCES = {"cufsp_plane.cuh": "cufsp_plane_src.inc", "cufsp_batch.cuh": "cufsp_batch_src.inc"}

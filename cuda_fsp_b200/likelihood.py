@@ -12,7 +12,7 @@ import math
 import numpy as np
 
 from . import _lib
-from ._lib import ModelDesc, SolverStatus
+from ._lib import AdaptiveStatus, ModelDesc, PROP_FACTOR_FN, SolverStatus
 from .fsp import FSPMat, MatrixFormat, _ptr, _stream
 
 
@@ -215,3 +215,64 @@ class Likelihood:
                                              C.byref(out), _stream(None)), "cufsp_loglik")
             ll += out.value + self.outside[it] * math.log(1e-44)
         return ll
+
+
+class AdaptiveFSP:
+    """FSP whose box grows until the FSP error (the probability that left the box) stays within
+    fsp_tol * t / t_last at every output time (cufsp_adaptive_*).  `model.factor(x, s, r)` gives the
+    propensity factors for any box; the model's bounds are the initial box."""
+
+    def __init__(self, model, max_bounds, times, fsp_tol: float = 1e-6, grow: float = 1.5, kry_tol: float = 1e-8,
+                 m: int = 30, coefs=None, lib=None):
+        import torch
+        if model.factor is None:
+            raise ValueError("AdaptiveFSP needs model.factor (propensity factors for any box)")
+        self._lib = lib or _lib.load()
+        self.model = model
+        d, self._keep = _model_desc(model)
+        d.factor_tables = None
+        self._cb = PROP_FACTOR_FN(lambda x, s, r: float(model.factor(x, s, r)))
+        d.prop_factor = self._cb
+        mb = np.ascontiguousarray(np.asarray(max_bounds, np.int32))
+        c = np.ascontiguousarray(np.asarray(model.coefs(0.0) if coefs is None else coefs, np.float64))
+        t = np.ascontiguousarray(np.asarray(times, np.float64))
+        self._h = C.c_void_p()
+        _lib.check(self._lib, self._lib.cufsp_adaptive_create(
+            C.byref(d), mb.ctypes.data_as(C.POINTER(C.c_int)), float(grow), float(fsp_tol),
+            c.ctypes.data_as(C.POINTER(C.c_double)), t.ctypes.data_as(C.POINTER(C.c_double)), len(t), float(kry_tol),
+            int(m), C.byref(self._h)), "cufsp_adaptive_create")
+        p0 = torch.as_tensor(model.p0(), device="cuda")
+        _lib.check(self._lib, self._lib.cufsp_adaptive_set_initial(self._h, p0.data_ptr(), _stream(None)),
+                   "cufsp_adaptive_set_initial")
+        torch.cuda.synchronize()
+
+    def next_time(self, stream=None) -> dict:
+        st = AdaptiveStatus()
+        _lib.check(self._lib, self._lib.cufsp_adaptive_next_time(self._h, _stream(stream), C.byref(st)),
+                   "cufsp_adaptive_next_time")
+        return st.as_dict()
+
+    def solution(self):
+        """(distribution on the current box as a device tensor (a copy), bounds)."""
+        import torch
+        ptr = C.c_void_p()
+        b = (C.c_int * self.model.ns)()
+        n = C.c_int64()
+        _lib.check(self._lib, self._lib.cufsp_adaptive_solution(self._h, C.byref(ptr), b, C.byref(n)),
+                   "cufsp_adaptive_solution")
+        out = torch.empty(n.value, dtype=torch.float64, device="cuda")
+        _lib.check(self._lib, self._lib.cufsp_vec_copy(n.value, ptr.value, out.data_ptr(), _stream(None)),
+                   "cufsp_vec_copy")
+        torch.cuda.synchronize()
+        return out, list(b)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            self._lib.cufsp_adaptive_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

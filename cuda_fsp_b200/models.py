@@ -34,6 +34,7 @@ class CMEModel:
     tcoef: Callable[[float], np.ndarray] | None = None   # c(t); None -> rates
     p0_kind: str = "delta0"              # "delta0" | "poisson5"
     meta: dict = field(default_factory=dict)
+    factor: Callable[[int, int, int], float] | None = None  # f_{r,s}(x) for any x (boxes of any size)
 
     @property
     def ns(self) -> int:
@@ -105,7 +106,13 @@ def mass_action(bounds, nu, orders, rates, name="mass_action", tcoef=None, p0_ki
         return v
 
     tables = _tables_from(bounds, nu.shape[0], fn)
-    return CMEModel(name, list(bounds), nu, tables, np.asarray(rates, np.float64), tcoef, p0_kind, meta or {})
+
+    def factor(x, s, r):  # the same falling factorial for a single count
+        v = 1.0
+        for j in range(int(orders[r, s])):
+            v *= max(x - j, 0.0)
+        return v
+    return CMEModel(name, list(bounds), nu, tables, np.asarray(rates, np.float64), tcoef, p0_kind, meta or {}, factor)
 
 
 # ---- the reference's toggle switch (tests/test_fsp_mat.cu:19-97, test_kry_expv.cu:80-106) ----
@@ -138,7 +145,9 @@ def toggle(bounds=(31, 31), time_varying=False) -> CMEModel:
         def tcoef(t):
             return np.array([p["kx0"], p["kx"] * (1.0 + math.cos(t / 1000.0)), p["dx"] * math.exp(-t / 3600.0),
                              p["ky0"], p["ky"], p["dy"] * math.exp(-t / 3600.0)])
-    return CMEModel("toggle", list(bounds), nu, _tables_from(bounds, 6, fn), rates, tcoef)
+    def factor(x, s, r):
+        return float(fn(np.array([float(x)]), s, r)[0])
+    return CMEModel("toggle", list(bounds), nu, _tables_from(bounds, 6, fn), rates, tcoef, factor=factor)
 
 
 def birth_death_2() -> CMEModel:

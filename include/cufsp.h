@@ -240,6 +240,36 @@ cufsp_status cufsp_solver_next_time(cufsp_solver *S, double *d_p, cufsp_stream_t
 cufsp_status cufsp_solver_solve(cufsp_solver *S, double *d_p, cufsp_stream_t stream, cufsp_solver_status *status);
 cufsp_status cufsp_solver_reset_time(cufsp_solver *S);
 
+/* ---- FSP with an adaptively grown box --------------------------------------------------------
+ * No counterpart in the reference: cme::FSPSolver stores fsp_tol but never uses it
+ * (src/FSPSolver.h:28).  The solver owns its distribution, since the box grows.  next_time() accepts
+ * the interval ending at times[i] only if the FSP error sum p(0) - sum p(times[i]) is at most
+ * fsp_tol * times[i] / times[last]; otherwise species whose upper face carries at least a tenth of
+ * the largest face mass grow by the factor `grow` (up to max_bounds), the generator is rebuilt from
+ * desc->prop_factor (required; evaluated on the host for every box), the distribution accepted at
+ * the previous output time is embedded and the interval is solved again (Krylov: m, kry_tol).
+ * When every species is at its maximum the solution is kept and fsp_tol_exceeded is set.
+ * coefs: host, n_reactions time-invariant rates.  Synchronous. */
+typedef struct {
+    int time_index;        /* output time reached */
+    double t;
+    double fsp_error;      /* probability that left the box by t */
+    int fsp_tol_exceeded;  /* the error is above its budget (box at its maximum) */
+    int expansions;        /* box enlargements so far */
+    int64_t n_states;      /* states of the current box */
+    int bounds[16];        /* current box (first n_species entries) */
+} cufsp_adaptive_status;
+typedef struct cufsp_adaptive_s cufsp_adaptive;
+cufsp_status cufsp_adaptive_create(const cufsp_model_desc *desc, const int *max_bounds, double grow, double fsp_tol,
+                                   const double *coefs, const double *times, int n_times, double kry_tol, int m,
+                                   cufsp_adaptive **out);
+cufsp_status cufsp_adaptive_destroy(cufsp_adaptive *S);
+/* d_p0: device, in the initial box (desc->fsp_bounds) */
+cufsp_status cufsp_adaptive_set_initial(cufsp_adaptive *S, const double *d_p0, cufsp_stream_t stream);
+cufsp_status cufsp_adaptive_next_time(cufsp_adaptive *S, cufsp_stream_t stream, cufsp_adaptive_status *status);
+/* The current distribution (device, owned by the solver, valid until the next call), box and size. */
+cufsp_status cufsp_adaptive_solution(const cufsp_adaptive *S, const double **d_p, int *bounds, int64_t *n_states);
+
 /* ---- likelihood and data generation ----------------------------------------------------------
  * One time point of Likelihood::evaluate (src/Likelihood.cpp:14-21):
  *   *out = sum_k counts[k] * log(max(1e-44, q[k])),  q[k] = sum_{j<block} p[k*block + j],
@@ -332,6 +362,9 @@ cufsp_status cufsp_expm_host(int k, const double *A, double *F);
 /* ---- vector helpers (device) ------------------------------------------------------------- */
 /* sum of x (deterministic order); result written to host *out; synchronises `stream`. */
 cufsp_status cufsp_vec_sum(int64_t n, const double *x, double *out, cufsp_stream_t stream);
+
+/* d_dst[0..n) = d_src[0..n) (device to device), ordered on `stream`. */
+cufsp_status cufsp_vec_copy(int64_t n, const double *d_src, double *d_dst, cufsp_stream_t stream);
 
 /* Sum of the n doubles at x (device), written to the device double *d_out, with NO device memory
  * allocated: no counterpart in the reference.  It is meant for callers that cannot call cudaMalloc
