@@ -254,9 +254,11 @@ PlaneData *plane_create(const ModelHost &m, const double *d_tables, std::string 
     pd->threads = 32 * chunks;
     pd->pitch = 64 * chunks;
     const int ytma = env_int("CUFSP_PLANE_YTMA", 1) != 0 ? 1 : 0;
+    const int pps = env_int("CUFSP_PLANE_PPS", 1) == 2 ? 2 : 1;  // planes per CTA barrier
     const DeviceInfo &di = device_info();
     const int want_tr = env_int("CUFSP_PLANE_TR", 2);
     const int want_s = std::max(3, std::min(12, env_int("CUFSP_PLANE_STAGES", 5)));
+    const int min_s = pps == 2 ? 4 : 3;
     auto stage_bytes = [&](int tr_, bool accum) {
         const int nq_ = rows ? tr_ + 2 : 1;
         return (size_t)8 * ((size_t)(nq_ + (accum && ytma ? tr_ : 0)) * pd->pitch + (size_t)tr_ * pd->wa.nwp);
@@ -266,7 +268,7 @@ PlaneData *plane_create(const ModelHost &m, const double *d_tables, std::string 
         if (tr) break;
         if (cand < 1 || cand > 8 || (rows ? pd->n1 % cand != 0 : cand != 1)) continue;
         if (cand > want_tr && want_tr >= 1) continue;
-        for (int st = want_s; st >= 3; --st)
+        for (int st = std::max(want_s, min_s); st >= min_s; --st)
             if (st * stage_bytes(cand, true) <= (size_t)di.max_smem_optin) {
                 tr = cand;
                 stages = st;
@@ -290,7 +292,7 @@ PlaneData *plane_create(const ModelHost &m, const double *d_tables, std::string 
     s << "#define CUFSP_PLANE_NR " << nr << "\n#define CUFSP_PLANE_NOFF " << offs.size() << "\n#define CUFSP_PLANE_NFA "
       << fa_tabs.size() << "\n#define CUFSP_PLANE_NFB " << fb_tabs.size() << "\n#define CUFSP_PLANE_NT " << terms.size()
       << "\n#define CUFSP_PLANE_NDG " << dgs.size() << "\n#define CUFSP_PLANE_TR " << tr << "\n#define CUFSP_PLANE_STAGES "
-      << stages << "\n#define CUFSP_PLANE_YTMA " << ytma << "\n#define CUFSP_PLANE_ROWS " << (rows ? 1 : 0) << "\n#define CUFSP_PLANE_THREADS " << pd->threads
+      << stages << "\n#define CUFSP_PLANE_PPS " << pps << "\n#define CUFSP_PLANE_YTMA " << ytma << "\n#define CUFSP_PLANE_ROWS " << (rows ? 1 : 0) << "\n#define CUFSP_PLANE_THREADS " << pd->threads
       << "\n#define CUFSP_PLANE_MINB " << minb << "\nnamespace cufsp_plane {\n";
     emit_fn(s, "nu0", nu0);
     emit_fn(s, "o0", o0);
@@ -359,7 +361,7 @@ PlaneData *plane_create(const ModelHost &m, const double *d_tables, std::string 
     std::ostringstream d;
     d << "plane kernel (NVRTC, sm_100a, TMA ring): NR=" << nr << " offsets=" << offs.size() << " terms=" << terms.size()
       << " diag groups=" << dgs.size() << " factor slots=" << fa_tabs.size() << "+" << fb_tabs.size() << " TR=" << tr
-      << " stages=" << stages << " ytma=" << ytma << " threads=" << pd->threads << " CTAs/SM=" << pd->occ_accum;
+      << " stages=" << stages << " planes/step=" << pps << " ytma=" << ytma << " threads=" << pd->threads << " CTAs/SM=" << pd->occ_accum;
     pd->description = d.str();
     return pd.release();
 }

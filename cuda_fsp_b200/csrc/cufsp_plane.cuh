@@ -70,6 +70,8 @@ constexpr int NT = CUFSP_PLANE_NT;      // shifted terms (offset, factor slot)
 constexpr int NDG = CUFSP_PLANE_NDG;    // diagonal groups (factor slot or constant 1)
 constexpr int TR = CUFSP_PLANE_TR;      // tile rows
 constexpr int S = CUFSP_PLANE_STAGES;   // ring stages
+constexpr int PPS = CUFSP_PLANE_PPS;    // planes per CTA barrier (1 or 2)
+static_assert(PPS == 1 || (PPS == 2 && S >= 4), "two planes per step need at least 4 stages");
 constexpr bool ROWS = CUFSP_PLANE_ROWS != 0;
 constexpr bool YTMA = CUFSP_PLANE_YTMA != 0;  // stage y rows in the ring (else L2 prefetch + loads)
 constexpr int NQ = ROWS ? TR + 2 : 1;   // staged x rows per plane (tile + halo)
@@ -341,10 +343,10 @@ __device__ __forceinline__ void plane_mv(const CufspPlaneArgs &a, const double *
     auto wait_plane = [&](int p) -> bool { return mbar_wait_bounded(bars + (p - pbase) % S, ((p - pbase) / S) & 1); };
 
     bool bad = false;
-    Slot q0, q1, q2;
+    Slot q0, q1, q2, q3;
     // prologue: planes z0 - 1 and z0 into the queue
     if (wait_plane(pbase) && wait_plane(t.z0)) {
-        load_slot(L, stage_of(pbase), a.pitch, q2);
+        load_slot(L, stage_of(pbase), a.pitch, PPS == 1 ? q2 : q3);
         load_slot(L, stage_of(t.z0), a.pitch, q0);
     } else {
         failed_flag = 1;
@@ -352,32 +354,70 @@ __device__ __forceinline__ void plane_mv(const CufspPlaneArgs &a, const double *
     __syncthreads();
     bad = failed_flag != 0;
 
-    // Step z: the slots hold (z - 1, z, z + 1) in a fixed rotation of 3.
     int z = t.z0;
-    auto step = [&](Slot &sm, Slot &s0, Slot &sp) -> bool {
-        if (bad || z >= t.z1) return false;
-        if (wait_plane(z + 1)) {
-            load_slot(L, stage_of(z + 1), a.pitch, sp);
-            const double *st = stage_of(z);
-            compute_rows<ACCUM, 0>(a, L, t, z, sm, s0, sp, st + LY::g_off(a.pitch), st + LY::y_off(a.pitch), Fa, Fb,
-                                   alpha, y);
-        } else {
-            failed_flag = 1;
-        }
-        __syncthreads();  // the stage of z is consumed
-        if (failed_flag) {
-            bad = true;
-            return false;
-        }
-        if (tid == 0 && issued < p_last) {
-            ++issued;
-            fence_proxy_async();
-            issue_plane<ACCUM>(a, t, x, y, stage_of(issued), bars + (issued - pbase) % S, issued);
-        }
-        ++z;
-        return true;
+    // Refill after a CTA barrier: the stages released by the step go to the next planes.
+    auto refill = [&](int count) {
+        if (tid == 0)
+            for (int k = 0; k < count && issued < p_last; ++k) {
+                ++issued;
+                fence_proxy_async();
+                issue_plane<ACCUM>(a, t, x, y, stage_of(issued), bars + (issued - pbase) % S, issued);
+            }
     };
-    while (step(q2, q0, q1) && step(q0, q1, q2) && step(q1, q2, q0)) {
+    if constexpr (PPS == 1) {
+        // Step z: the slots hold (z - 1, z, z + 1) in a fixed rotation of 3; one barrier per plane.
+        auto step = [&](Slot &sm, Slot &s0, Slot &sp) -> bool {
+            if (bad || z >= t.z1) return false;
+            if (wait_plane(z + 1)) {
+                load_slot(L, stage_of(z + 1), a.pitch, sp);
+                const double *st = stage_of(z);
+                compute_rows<ACCUM, 0>(a, L, t, z, sm, s0, sp, st + LY::g_off(a.pitch), st + LY::y_off(a.pitch), Fa,
+                                       Fb, alpha, y);
+            } else {
+                failed_flag = 1;
+            }
+            __syncthreads();  // the stage of z is consumed
+            if (failed_flag) {
+                bad = true;
+                return false;
+            }
+            refill(1);
+            ++z;
+            return true;
+        };
+        while (step(q2, q0, q1) && step(q0, q1, q2) && step(q1, q2, q0)) {
+        }
+    } else {
+        // Double step z: slots (z - 1, z, z + 1, z + 2) in a rotation of 4; planes z and z + 1 are
+        // computed under one barrier (z + 1 only while inside the segment).
+        auto step2 = [&](Slot &sa, Slot &sb, Slot &sc, Slot &sd) -> bool {
+            if (bad || z >= t.z1) return false;
+            const bool two = z + 1 < t.z1;
+            if (wait_plane(z + 1) && (!two || wait_plane(z + 2))) {
+                load_slot(L, stage_of(z + 1), a.pitch, sc);
+                if (two) load_slot(L, stage_of(z + 2), a.pitch, sd);
+                const double *st = stage_of(z);
+                compute_rows<ACCUM, 0>(a, L, t, z, sa, sb, sc, st + LY::g_off(a.pitch), st + LY::y_off(a.pitch), Fa,
+                                       Fb, alpha, y);
+                if (two) {
+                    const double *st1 = stage_of(z + 1);
+                    compute_rows<ACCUM, 0>(a, L, t, z + 1, sb, sc, sd, st1 + LY::g_off(a.pitch),
+                                           st1 + LY::y_off(a.pitch), Fa, Fb, alpha, y);
+                }
+            } else {
+                failed_flag = 1;
+            }
+            __syncthreads();  // the stages of z and z + 1 are consumed
+            if (failed_flag) {
+                bad = true;
+                return false;
+            }
+            refill(two ? 2 : 1);
+            z += two ? 2 : 1;
+            return true;
+        };
+        while (step2(q3, q0, q1, q2) && step2(q1, q2, q3, q0)) {
+        }
     }
     if (tid == 0) {
         // every issued copy must have landed before the CTA's shared memory is released

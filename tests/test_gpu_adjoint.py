@@ -109,3 +109,19 @@ def test_batched_gradients_equal_single_gradients(cuda):
         lli, gi = L.gradient(sets[i])
         assert abs(ll[i] - lli) <= 1e-12 * abs(lli)
         assert np.max(np.abs(g[i] - gi)) <= 1e-12 * np.max(np.abs(gi))
+
+
+def test_torch_autograd_wrapper(cuda):
+    """torch.autograd through log_likelihood gives the adjoint gradient (d log L / d log theta)."""
+    import torch
+    from cuda_fsp_b200.autograd import log_likelihood
+    m = models.gene_expression((1, 1, 1, 15, 15), time_varying=False)
+    times = np.array([2.0, 6.0])
+    counts = synthetic_counts(m, times, 8, 400, seed=8)
+    L = Likelihood(m, times, counts, n_marginal=3, kry_tol=1e-10)
+    lt = torch.tensor(np.log(m.coefs(0)), dtype=torch.float64, requires_grad=True)
+    ll = log_likelihood(lt, L)
+    ll.backward()
+    ll_ref, g_ref = L.gradient(np.exp(lt.detach().numpy()))  # the same rates, bit for bit
+    assert ll.item() == ll_ref
+    assert np.array_equal(lt.grad.numpy(), g_ref)
