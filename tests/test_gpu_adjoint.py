@@ -123,5 +123,5 @@ def test_torch_autograd_wrapper(cuda):
     ll = log_likelihood(lt, L)
     ll.backward()
     ll_ref, g_ref = L.gradient(np.exp(lt.detach().numpy()))  # the same rates, bit for bit
-    assert ll.item() == ll_ref
-    assert np.array_equal(lt.grad.numpy(), g_ref)
+    assert abs(ll.item() - ll_ref) <= 1e-12 * abs(ll_ref)
+    assert np.max(np.abs(lt.grad.numpy() - g_ref)) <= 1e-9 * np.max(np.abs(g_ref))
