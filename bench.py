@@ -168,6 +168,37 @@ def cpu_oracle_gbs(min_steps: int, warmup: int, bounds=CPU_SAMPLE_BOUNDS, budget
             "ms_per_step": dt * 1e3}
 
 
+def reference_gpu_kernel() -> dict | None:
+    """The reference's own Kronecker action (fspmat_sdkron_mv through SDKronMatSet::action,
+    src/fspmat_kron_kernels.cu:31-129, built unmodified for sm_100a into oracle/_ref) on the full
+    255^3 workload: a reported baseline beside the CPU one, None without a GPU or the build."""
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return None
+    except Exception:
+        return None
+    import oracle
+    from cuda_fsp_b200 import models
+    R = oracle.ref()
+    if R is None:
+        return None
+    m = models.mass_action_3()
+    b = np.asarray(m.bounds, np.int32)
+    sv, sc, sr = m.stoich_csr()
+    tab = np.ascontiguousarray(m.tables)
+    c = np.ascontiguousarray(m.coefs(0))
+    ms = R.ref_gpu_kron_time(m.ns, m.nr, b.ctypes.data, sv.ctypes.data, sc.ctypes.data, sr.ctypes.data,
+                             tab.ctypes.data, c.ctypes.data, 100)
+    if ms <= 0:
+        return None
+    return {"value": round(BYTES_PER_STATE * m.n_states / (ms * 1e-3) / 1e9, 3), "unit": "GB/s",
+            "ms_per_action": round(ms, 4),
+            "kernel": "reference fspmat_sdkron_mv built for sm_100a, called through SDKronMatSet::action "
+                      "(coefficient copy and device synchronisation per call, as the reference does); "
+                      "100 actions (the count of the reference's benchmark_fsp_mat.cu:158), CUDA events, x and y resident"}
+
+
 def run_reference(args):
     world, rank, _ = dist_setup()
     if rank != 0:
@@ -180,6 +211,9 @@ def run_reference(args):
             "data": "synthetic", "config": {"workload": WORKLOAD, "sample": cb["sample"]},
             "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
             "e2e": {"value": round(cb["value"], 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    gk = reference_gpu_kernel()
+    if gk is not None:
+        line["reference_gpu_kernel"] = gk
     print(json.dumps(line), flush=True)
 
 
@@ -204,6 +238,50 @@ def expmv_secondary() -> dict:
     return {"metric": "expmv solves/s", "workload": "birth_death_2, 32,768 states, t = 10, m = 30, tol 1e-8",
             "value": round(1.0 / dt, 3), "ms_per_solve": round(dt * 1e3, 3), "krylov_steps": st["n_steps"],
             "matvecs": st["n_matvec"]}
+
+
+def expmv_large_secondary(max_steps: int = 400, budget_s: float = 12.0) -> dict:
+    """Krylov exp(tA)p0 on the 255^3 workload (mass_action_3, p0 = Poisson(5)^3, t = 20, m = 30,
+    tol 1e-8, full orthogonalisation) over a bounded sample of its steps: Krylov steps per second
+    and the Arnoldi traffic rate against the HBM roofline.  The whole solve takes ~3e4 steps (the
+    x1 x2 and x1 x3 propensities make it stiff), too long for a benchmark run, so the sample is the
+    first steps from p0.  Algorithmic bytes per step (minimum fused traffic of one step with
+    overwrite-form matvecs): (16 (m+1) + 8 (m (m+1) + 2m) + 8 (m+2)) n = 8,672 n."""
+    import torch
+    from cuda_fsp_b200 import FSPMat, KryExpvFSP, MatrixFormat, models
+    mm = models.mass_action_3()
+    n = mm.n_states
+    A = FSPMat.from_model(mm, MatrixFormat.KRONECKER)
+    v = torch.as_tensor(mm.p0(), device="cuda")
+    E = KryExpvFSP(20.0, A, v, m=30, tol=1e-8, coefs=mm.coefs(0))
+    E.max_nstep = 1 << 20
+    for _ in range(3):  # graph capture and warm-up
+        E.step()
+    st0 = E.stats
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    k = 0
+    while k < max_steps and not E.final_time_reached():
+        E.step()
+        k += 1
+        if k % 20 == 0:
+            torch.cuda.synchronize()
+            if time.perf_counter() - t0 > budget_s:
+                break
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    st = E.stats
+    steps = st["n_steps"] - st0["n_steps"]
+    bps = (16 * 31 + 8 * (30 * 31 + 60) + 8 * 32) * n
+    gbs = steps * bps / dt / 1e9
+    peak, _ = measured_peak_hbm()
+    return {"metric": "expmv Krylov steps/s", "workload": "mass_action_3 255^3 = 16,777,216 states, p0 = Poisson(5)^3, "
+                                                          "t = 20, m = 30, tol 1e-8, full orthogonalisation",
+            "value": round(steps / dt, 3), "ms_per_step": round(dt / steps * 1e3, 3), "steps_timed": steps,
+            "t_reached": round(st["t_now"], 5), "t_final": 20.0,
+            "matvecs_per_step": round((st["n_matvec"] - st0["n_matvec"]) / steps, 2),
+            "arnoldi_bytes_per_step": bps, "achieved_gbs": round(gbs, 1), "frac_of_measured_hbm": round(gbs / peak, 4),
+            "mass": round(v.sum().item(), 12)}
 
 
 def cpu_expmv_ms() -> float:
@@ -409,7 +487,7 @@ def run_ours(args):
     elif rank == 0:
         secondary = expmv_secondary()
         secondary["cpu_oracle_ms_per_solve"] = round(cpu_expmv_ms(), 1)
-        secondary = [secondary, batched_secondary(), gradient_secondary()]
+        secondary = [secondary, expmv_large_secondary(), batched_secondary(), gradient_secondary()]
     cpu = cpu_oracle_gbs(max(3, min(args.steps, 20)), 1) if (rank == 0 and world == 1) else None
     peak, peak_kind = measured_peak_hbm()
     if rank == 0:

@@ -246,10 +246,11 @@ PlaneData *plane_create(const ModelHost &m, const double *d_tables, std::string 
         pd->wa.r_term[r] = r_term[r];
         pd->wa.r_dg[r] = r_dg[r];
     }
-    // tile rows (dividing n1) and ring stages
-    // Tile rows TR (dividing n1) and ring stages S: the preferred pair (TR = 2, S = 5 unless set by
-    // CUFSP_PLANE_TR / CUFSP_PLANE_STAGES), stepping down -- fewer stages first, then lower tiles --
-    // until the ring fits the shared memory of one SM.
+    // Tile rows TR (dividing n1; 2 unless CUFSP_PLANE_TR says otherwise, stepping down when nothing
+    // fits) and ring stages S (3..5, or exactly CUFSP_PLANE_STAGES when set).  Occupancy comes first:
+    // among the stage counts that fit, take the one giving the most CTAs per SM -- bounded by the
+    // ring's shared memory and by 128 registers per thread -- and the most stages among those.
+    // (At 255^3: S = 4 with 4 CTAs/SM moves 5.2 TB/s where S = 5 with 3 CTAs/SM moves 4.85.)
     const int chunks = (n0 + 63) / 64;
     pd->threads = 32 * chunks;
     pd->pitch = 64 * chunks;
@@ -257,23 +258,39 @@ PlaneData *plane_create(const ModelHost &m, const double *d_tables, std::string 
     const int pps = env_int("CUFSP_PLANE_PPS", 1) == 2 ? 2 : 1;  // planes per CTA barrier
     const DeviceInfo &di = device_info();
     const int want_tr = env_int("CUFSP_PLANE_TR", 2);
-    const int want_s = std::max(3, std::min(12, env_int("CUFSP_PLANE_STAGES", 5)));
+    const int env_s = env_int("CUFSP_PLANE_STAGES", 0);
     const int min_s = pps == 2 ? 4 : 3;
+    const int max_s = env_s > 0 ? std::max(min_s, std::min(12, env_s)) : 5;
     auto stage_bytes = [&](int tr_, bool accum) {
         const int nq_ = rows ? tr_ + 2 : 1;
         return (size_t)8 * ((size_t)(nq_ + (accum && ytma ? tr_ : 0)) * pd->pitch + (size_t)tr_ * pd->wa.nwp);
+    };
+    const int by_regs = std::max(1, 65536 / (128 * pd->threads));
+    auto ctas_per_sm = [&](size_t smem) {
+        return std::min(by_regs, (int)std::max<size_t>(1, (size_t)(di.max_smem_optin + 1024) / (smem + 1024)));
     };
     int tr = 0, stages = 0;
     for (int cand : {want_tr, 4, 2, 1}) {
         if (tr) break;
         if (cand < 1 || cand > 8 || (rows ? pd->n1 % cand != 0 : cand != 1)) continue;
         if (cand > want_tr && want_tr >= 1) continue;
-        for (int st = std::max(want_s, min_s); st >= min_s; --st)
-            if (st * stage_bytes(cand, true) <= (size_t)di.max_smem_optin) {
+        int best_occ = 0;
+        for (int st = max_s; st >= (env_s > 0 ? max_s : min_s); --st) {
+            const size_t b = st * stage_bytes(cand, true);
+            if (b > (size_t)di.max_smem_optin) continue;
+            const int occ = ctas_per_sm(b);
+            if (occ > best_occ) {
+                best_occ = occ;
                 tr = cand;
                 stages = st;
-                break;
             }
+        }
+        if (!tr && env_s > 0)  // the requested stage count does not fit: step down as far as needed
+            for (int st = max_s - 1; st >= min_s && !tr; --st)
+                if (st * stage_bytes(cand, true) <= (size_t)di.max_smem_optin) {
+                    tr = cand;
+                    stages = st;
+                }
     }
     if (!tr) {
         why = "ring stages exceed shared memory";
@@ -283,11 +300,8 @@ PlaneData *plane_create(const ModelHost &m, const double *d_tables, std::string 
     pd->row_blocks = pd->n1 / tr;
     pd->smem_accum = stages * stage_bytes(tr, true);
     pd->smem_set = stages * stage_bytes(tr, false);
-    // CTAs per SM the launch bounds promise: as many as the ring stages fit in shared memory, but
-    // never so many that a thread gets fewer than 128 registers.
-    const int by_smem = (int)std::max<size_t>(1, (size_t)(di.max_smem_optin + 1024) / (pd->smem_accum + 1024));
-    const int by_regs = std::max(1, 65536 / (128 * pd->threads));
-    const int minb = std::max(1, std::min(16, env_int("CUFSP_PLANE_MINB", std::min(by_smem, by_regs))));
+    // CTAs per SM the launch bounds promise (the occupancy the shape was chosen for).
+    const int minb = std::max(1, std::min(16, env_int("CUFSP_PLANE_MINB", ctas_per_sm(pd->smem_accum))));
     std::ostringstream s;
     s << "#define CUFSP_PLANE_NR " << nr << "\n#define CUFSP_PLANE_NOFF " << offs.size() << "\n#define CUFSP_PLANE_NFA "
       << fa_tabs.size() << "\n#define CUFSP_PLANE_NFB " << fb_tabs.size() << "\n#define CUFSP_PLANE_NT " << terms.size()
