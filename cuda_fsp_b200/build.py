@@ -26,9 +26,12 @@ OBJ = PKG / "_build"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-rdc=true", "-Xcompiler", "-fPIC,-O2",
                      "-I" + str(ROOT / "include"), "--expt-relaxed-constexpr", "--extended-lambda"]
+# The small dense kernels of the host Pade exponential vectorise at -O3 only.
+HOST_EXTRA = {"cufsp_expm.cpp": ["-Xcompiler", "-O3"]}
 SOURCES = ["cufsp_common.cu", "cufsp_kron.cu", "cufsp_kron_plane.cu", "cufsp_kron_march.cu", "cufsp_sparse.cu", "cufsp_mat.cu",
            "cufsp_krylov.cu", "cufsp_expm.cpp", "cufsp_noalloc.cu", "cufsp_stats.cu", "cufsp_solver.cu",
-           "cufsp_vec.cu", "cufsp_bdf.cu", "cufsp_batch.cu", "cufsp_adjoint.cu", "cufsp_adaptive.cu"]
+           "cufsp_vec.cu", "cufsp_bdf.cu", "cufsp_batch.cu", "cufsp_adjoint.cu", "cufsp_adaptive.cu",
+           "cufsp_arnoldi.cu"]
 HEADERS = ["cufsp_internal.h", "cufsp_reduce.cuh", "cufsp_march.h", "cufsp_vec.h", "cufsp_plane.cuh", "cufsp_batch.cuh"]
 # Kernel sources compiled at run time by NVRTC are embedded in the library as string literals.
 RTC_SOURCES = {"cufsp_plane.cuh": "cufsp_plane_src.inc", "cufsp_batch.cuh": "cufsp_batch_src.inc"}
@@ -90,7 +93,7 @@ def build(force: bool = False, verbose: bool = False) -> dict[str, Path]:
     if cpp_test.exists():
         jobs.append((cpp_test, OBJ / "test_dropin.cu.o"))
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 4)) as ex:
-        objs = list(ex.map(lambda j: _compile(j[0], j[1], [], force), jobs))
+        objs = list(ex.map(lambda j: _compile(j[0], j[1], HOST_EXTRA.get(j[0].name, []), force), jobs))
     lib_objs = [str(o) for o in objs[: len(srcs)]]
     out = {}
     so = LIB / "libcufsp.so"

@@ -464,6 +464,7 @@ extern "C" cufsp_status cufsp_likelihood_grad_batched(const cufsp_model_desc *de
     std::vector<std::string> msg(workers);
     auto work = [&](int w) {
         cudaSetDevice(dev);
+        parnoldi_thread_disable(workers > 1);
         cufsp_mat *A = nullptr;
         cudaStream_t st = nullptr;
         cufsp_status s = cufsp_mat_create(desc, CUFSP_FORMAT_KRONECKER, &A);
@@ -482,6 +483,7 @@ extern "C" cufsp_status cufsp_likelihood_grad_batched(const cufsp_model_desc *de
         }
         if (st) cudaStreamDestroy(st);
         cufsp_mat_destroy(A);
+        parnoldi_thread_disable(false);
     };
     std::vector<std::thread> pool;
     for (int w = 1; w < workers; ++w) pool.emplace_back(work, w);

@@ -18,9 +18,32 @@ namespace cufsp {
 
 namespace {
 
-void matmul(int k, const double *__restrict A, const double *__restrict B, double *__restrict C) {
-    // C = A * B, column-major; loop order j-l-i keeps the inner loop unit-stride (vectorisable).
-    for (int j = 0; j < k; ++j) {
+// C = A * B, column-major, four columns of C per pass over A (the inner loop is unit-stride).
+// Cloned for AVX-512, AVX2 and baseline x86-64; the loader picks the widest the host supports.
+__attribute__((target_clones("avx512f", "avx2", "default"))) void matmul(int k, const double *__restrict A,
+                                                                         const double *__restrict B,
+                                                                         double *__restrict C) {
+    int j = 0;
+    for (; j + 4 <= k; j += 4) {
+        double *__restrict c0 = C + (size_t)j * k;
+        double *__restrict c1 = c0 + k;
+        double *__restrict c2 = c1 + k;
+        double *__restrict c3 = c2 + k;
+        for (int i = 0; i < k; ++i) c0[i] = c1[i] = c2[i] = c3[i] = 0.0;
+        for (int l = 0; l < k; ++l) {
+            const double b0 = B[l + (size_t)j * k], b1 = B[l + (size_t)(j + 1) * k];
+            const double b2 = B[l + (size_t)(j + 2) * k], b3 = B[l + (size_t)(j + 3) * k];
+            const double *__restrict al = A + (size_t)l * k;
+            for (int i = 0; i < k; ++i) {
+                const double a = al[i];
+                c0[i] += a * b0;
+                c1[i] += a * b1;
+                c2[i] += a * b2;
+                c3[i] += a * b3;
+            }
+        }
+    }
+    for (; j < k; ++j) {
         double *__restrict cj = C + (size_t)j * k;
         for (int i = 0; i < k; ++i) cj[i] = 0.0;
         for (int l = 0; l < k; ++l) {

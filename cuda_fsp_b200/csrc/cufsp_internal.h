@@ -181,6 +181,20 @@ cufsp_status mat_prepare(cufsp_mat *A, const double *coefs, cudaStream_t st);
 cufsp_status mat_apply_transpose(cufsp_mat *A, const double *coefs, double alpha, const double *d_alpha,
                                  const int *d_skip, const double *x, double *y, cudaStream_t st);
 
+// Persistent single-launch Arnoldi pass for generators whose Krylov basis stays in L2
+// (cufsp_arnoldi.cu).  Writes the same device state block as the launch sequence of
+// cufsp_krylov.cu; *err (zeroed here) is set when a bounded grid-barrier wait expired.
+struct PArnoldi;
+bool parnoldi_wanted(const cufsp_mat *A, int64_t n, int m);
+cufsp_status parnoldi_run(PArnoldi **pa, cufsp_mat *A, const std::vector<double> &coefs, bool transpose,
+                          int64_t n, const double *v, double *W, double *H, double *rho, double *gam, double *beta,
+                          double *avnorm, int *flag, int *err, int m, int iop, int q, double btol, bool with_avnorm,
+                          cudaStream_t st);
+void parnoldi_destroy(PArnoldi *pa);
+// Host threads that run solves concurrently with other threads keep the launch sequence: the
+// persistent pass wants every SM to itself.
+void parnoldi_thread_disable(bool off);
+
 // Internals of the single-instance Krylov driver used by the adjoint gradient (cufsp_krylov.cu).
 void expv_set_transpose(cufsp_expv *E, bool transpose);
 cufsp_status expv_arnoldi(cufsp_expv *E, double *v, cudaStream_t st);  // Arnoldi pass only

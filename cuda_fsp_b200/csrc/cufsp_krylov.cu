@@ -209,6 +209,7 @@ struct cufsp_expv_s {
     };
     std::vector<Graph> graphs;
     cudaStream_t cap_stream = nullptr;
+    cufsp::PArnoldi *pa = nullptr;  // persistent single-launch Arnoldi pass (small generators)
 };
 
 namespace {
@@ -300,7 +301,13 @@ bool graphs_enabled() {
 // step); the generator's coefficient-dependent tables are prepared eagerly before each replay.
 cufsp_status arnoldi_pass(cufsp_expv *E, double *v, cudaStream_t st, bool with_avnorm) {
     cufsp_status s;
-    if (E->A && graphs_enabled()) {
+    const bool persistent = E->A && parnoldi_wanted(E->A, E->n, E->m);
+    if (persistent) {
+        s = parnoldi_run(&E->pa, E->A, E->coefs, E->transpose, E->n, v, E->W, E->ks.H, E->ks.rho, E->ks.gam,
+                         E->ks.beta, E->ks.avnorm, E->ks.flag, E->ks.flag + 1, E->m, E->iop, E->q_iop, E->btol,
+                         with_avnorm, st);
+        if (s != CUFSP_SUCCESS) return s;
+    } else if (E->A && graphs_enabled()) {
         s = mat_prepare(E->A, E->coefs.data(), st);
         if (s != CUFSP_SUCCESS) return s;
         cudaGraphExec_t exec = nullptr;
@@ -338,8 +345,11 @@ cufsp_status arnoldi_pass(cufsp_expv *E, double *v, cudaStream_t st, bool with_a
     const int mp2 = m + 2;
     const double *hH = E->hstate.data();
     const double *hrho = hH + (size_t)mp2 * mp2;
-    int flag;
+    int flag, barrier_err;
     std::memcpy(&flag, hrho + 2 * mp2 + 4, sizeof(int));
+    std::memcpy(&barrier_err, reinterpret_cast<const char *>(hrho + 2 * mp2 + 4) + sizeof(int), sizeof(int));
+    if (persistent && barrier_err)
+        return set_error(CUFSP_ERR_CUDA, "expv: a grid barrier wait of the persistent Arnoldi pass expired");
     KrylovStep &L = E->last;
     L.mb = flag > 0 ? flag : m;
     L.beta = hrho[2 * mp2];
@@ -528,6 +538,7 @@ extern "C" cufsp_status cufsp_expv_create(int64_t n, int m, double tol, int iop,
 extern "C" cufsp_status cufsp_expv_destroy(cufsp_expv *E) {
     if (!E) return CUFSP_SUCCESS;
     for (auto &g : E->graphs) cudaGraphExecDestroy(g.exec);
+    parnoldi_destroy(E->pa);
     if (E->cap_stream) cudaStreamDestroy(E->cap_stream);
     if (E->W) cudaFree(E->W);
     if (E->d_state) cudaFree(E->d_state);
@@ -553,6 +564,10 @@ extern "C" cufsp_status cufsp_expv_bind_mat_coefs(cufsp_expv *E, cufsp_mat *A, c
     // graphs hold the operator's launch parameters (coefficients included): rebuild them
     for (auto &g : E->graphs) cudaGraphExecDestroy(g.exec);
     E->graphs.clear();
+    if (E->A != A) {  // the persistent pass keeps the generator's model data
+        parnoldi_destroy(E->pa);
+        E->pa = nullptr;
+    }
     E->A = A;
     E->fn = nullptr;
     return CUFSP_SUCCESS;
