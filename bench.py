@@ -360,12 +360,13 @@ def batched_sharded_secondary(world: int, rank: int, dev, per_rank: int = 256) -
             "s_per_batch": round(dt.item(), 3), "scaling": "weak", "failed": sum(1 for r in res if r["status"] != 0)}
 
 
-def gradient_secondary(n_sets: int = 16, workers: int = 16) -> dict:
+def gradient_secondary(n_sets: int = 64, workers: int = 2) -> dict:
     """C5: d log L / d log theta for the 12 rates of the gene-expression model (131,072 states) from
     1,000 seeded-SSA cells at 8 log-spaced times in [1, 60], (n, c) histograms marginalised over the
     gene states, for n_sets parameter sets (rates within half a decade of nominal) at once
-    (cufsp_likelihood_grad_batched, `workers` concurrent adjoint solves); one single-set gradient and
-    one log-likelihood evaluation are timed beside it."""
+    (cufsp_likelihood_grad_batched: `workers` concurrent adjoint solves; at this size each solve's
+    Arnoldi passes fill the GPU, so two workers overlap one solve's passes with the other's host-side
+    step control); one single-set gradient and one log-likelihood evaluation are timed beside it."""
     import torch
     from cuda_fsp_b200 import Likelihood, generate_data, histograms, models
     m = models.gene_expression((1, 1, 1, 127, 127), time_varying=False)

@@ -453,10 +453,18 @@ extern "C" cufsp_status cufsp_likelihood_grad_batched(const cufsp_model_desc *de
                                                       int64_t block, const double *d_counts, int m, double tol,
                                                       int workers, double *logL, double *grad) {
     clear_error();
-    if (!desc || !coefs || !logL || !grad || n_sets < 1)
+    if (!desc || !desc->fsp_bounds || desc->n_species < 1 || desc->n_species > CUFSP_MAX_SPECIES || !coefs || !logL ||
+        !grad || n_sets < 1)
         return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_likelihood_grad_batched: bad argument");
     const int nr = desc->n_reactions;
     workers = std::max(1, std::min(std::min(workers, n_sets), 32));
+    // Generators small enough for the persistent Arnoldi pass: one such pass fills the GPU, so two
+    // workers suffice (one solve's pass overlaps the other's host-side step control); larger
+    // generators run `workers` concurrent launch sequences.
+    int64_t n_states = 1;
+    for (int s = 0; s < desc->n_species; ++s) n_states *= (int64_t)desc->fsp_bounds[s] + 1;
+    const bool persistent = parnoldi_size_ok(n_states);
+    if (persistent) workers = std::min(workers, 2);
     int dev = 0;
     CUFSP_CUDA_TRY(cudaGetDevice(&dev));
     std::atomic<int> next(0);
@@ -464,7 +472,7 @@ extern "C" cufsp_status cufsp_likelihood_grad_batched(const cufsp_model_desc *de
     std::vector<std::string> msg(workers);
     auto work = [&](int w) {
         cudaSetDevice(dev);
-        parnoldi_thread_disable(workers > 1);
+        parnoldi_thread_disable(!persistent && workers > 1);
         cufsp_mat *A = nullptr;
         cudaStream_t st = nullptr;
         cufsp_status s = cufsp_mat_create(desc, CUFSP_FORMAT_KRONECKER, &A);

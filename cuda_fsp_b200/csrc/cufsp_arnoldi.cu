@@ -366,20 +366,29 @@ void parnoldi_destroy(PArnoldi *pa) {
 
 void parnoldi_thread_disable(bool off) { tl_disabled = off; }
 
-bool parnoldi_wanted(const cufsp_mat *A, int64_t n, int m) {
+namespace {
+int persistent_mode() {  // CUFSP_ARNOLDI_PERSISTENT: 0 never, 1 always, unset: by size
     static const int mode = [] {
         const char *e = getenv("CUFSP_ARNOLDI_PERSISTENT");
-        return e ? atoi(e) : -1;  // -1: by size
+        return e ? atoi(e) : -1;
     }();
+    return mode;
+}
+}  // namespace
+
+bool parnoldi_size_ok(int64_t n) {
     static const int64_t max_n = [] {
         const char *e = getenv("CUFSP_ARNOLDI_MAX_N");
         return e ? (int64_t)atoll(e) : (int64_t)1 << 20;
     }();
-    if (mode == 0 || tl_disabled || !A || m > CUFSP_MAX_KRYLOV) return false;
+    const int mode = persistent_mode();
+    return mode != 0 && (mode == 1 || n <= max_n);
+}
+
+bool parnoldi_wanted(const cufsp_mat *A, int64_t n, int m) {
+    if (tl_disabled || !A || m > CUFSP_MAX_KRYLOV || !parnoldi_size_ok(n)) return false;
     if (A->model.nr > CUFSP_MAX_REACTIONS_SPARSE || A->model.ns > CUFSP_MAX_SPECIES) return false;
-    if (A->format == CUFSP_FORMAT_KRONECKER ? A->model.tables.empty() : !A->sparse) return false;
-    if (mode == 1) return true;
-    return n <= max_n;
+    return A->format == CUFSP_FORMAT_KRONECKER ? !A->model.tables.empty() : A->sparse != nullptr;
 }
 
 namespace {

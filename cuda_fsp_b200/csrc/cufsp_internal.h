@@ -186,13 +186,14 @@ cufsp_status mat_apply_transpose(cufsp_mat *A, const double *coefs, double alpha
 // cufsp_krylov.cu; *err (zeroed here) is set when a bounded grid-barrier wait expired.
 struct PArnoldi;
 bool parnoldi_wanted(const cufsp_mat *A, int64_t n, int m);
+bool parnoldi_size_ok(int64_t n);  // the size rule of parnoldi_wanted alone
 cufsp_status parnoldi_run(PArnoldi **pa, cufsp_mat *A, const std::vector<double> &coefs, bool transpose,
                           int64_t n, const double *v, double *W, double *H, double *rho, double *gam, double *beta,
                           double *avnorm, int *flag, int *err, int m, int iop, int q, double btol, bool with_avnorm,
                           cudaStream_t st);
 void parnoldi_destroy(PArnoldi *pa);
-// Host threads that run solves concurrently with other threads keep the launch sequence: the
-// persistent pass wants every SM to itself.
+// Host threads that run many solves concurrently keep the launch sequence: the persistent pass
+// wants every SM to itself.
 void parnoldi_thread_disable(bool off);
 
 // Internals of the single-instance Krylov driver used by the adjoint gradient (cufsp_krylov.cu).
