@@ -284,6 +284,41 @@ def expmv_large_secondary(max_steps: int = 400, budget_s: float = 12.0) -> dict:
             "mass": round(v.sum().item(), 12)}
 
 
+def bdf_secondary() -> dict:
+    """C2: the time-varying gene-expression model (131,072 states, switching rate
+    k0 sigmoid((t - 5) / 0.5)) from p0 to t = 60 by the device BDF integrator (rtol 1e-8, atol 1e-14;
+    the reference's CVODE path).  The oracle's host BDF is timed on the sample [0, 6] (the switch and
+    408 of the ~700 steps), with the device solve of the same sample beside it."""
+    import torch
+    import oracle
+    from cuda_fsp_b200 import BDFIntegrator, FSPMat, MatrixFormat, models
+    m = models.gene_expression((1, 1, 1, 127, 127), time_varying=True)
+    A = FSPMat.from_model(m, MatrixFormat.KRONECKER)
+    p0 = torch.as_tensor(m.p0(), device="cuda")
+
+    def solve(t_end):
+        B = BDFIntegrator(A, rtol=1e-8, atol=1e-14)
+        p = p0.clone()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        B.init(0.0, p)
+        B.advance(t_end, p)
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0, B.stats, p
+
+    solve(6.0)  # warm-up
+    full, st, p = solve(60.0)
+    sample, st6, _ = solve(6.0)
+    t0 = time.perf_counter()
+    _, rst, rc = oracle.bdf(oracle.assemble_model(m), m.coefs, 0.0, m.p0(), [6.0], rtol=1e-8, atol=1e-14)
+    cpu = time.perf_counter() - t0
+    return {"metric": "BDF solve s", "workload": "gene_expression 131,072 states, time-varying switch, t = 60, "
+            "rtol 1e-8, atol 1e-14", "value": round(full, 4), "steps": st["n_steps"], "order": st["order"],
+            "mass": round(p.sum().item(), 12), "sample_t6_s": round(sample, 4), "sample_t6_steps": st6["n_steps"],
+            "cpu_oracle_sample_t6_s": round(cpu, 3), "cpu_oracle_sample_t6_steps": rst["n_steps"],
+            "cpu_oracle_rc": rc}
+
+
 def cpu_expmv_ms() -> float:
     """The oracle's host Krylov exp(tA)v on birth_death_2 (same workload as the expmv leg)."""
     import oracle
@@ -488,7 +523,7 @@ def run_ours(args):
     elif rank == 0:
         secondary = expmv_secondary()
         secondary["cpu_oracle_ms_per_solve"] = round(cpu_expmv_ms(), 1)
-        secondary = [secondary, expmv_large_secondary(), batched_secondary(), gradient_secondary()]
+        secondary = [secondary, bdf_secondary(), expmv_large_secondary(), batched_secondary(), gradient_secondary()]
     cpu = cpu_oracle_gbs(max(3, min(args.steps, 20)), 1) if (rank == 0 and world == 1) else None
     peak, peak_kind = measured_peak_hbm()
     if rank == 0:

@@ -495,10 +495,14 @@ cufsp_status parnoldi_run(PArnoldi **ppa, cufsp_mat *A, const std::vector<double
     cufsp_status s = build_terms(pa, A, coefs, transpose, tm, st);
     if (s != CUFSP_SUCCESS) return s;
     if (!pa->grid) {
-        // One CTA per SM (fewer for small n: at least 256 states each); the CTA's slice of the
-        // newest vector must fit its shared memory.
+        // One CTA per SM (fewer for small n: at least 256 states each by default); the CTA's slice
+        // of the newest vector must fit its shared memory.
+        static const int64_t min_states = [] {  // states per CTA at least (CUFSP_ARNOLDI_CTA_STATES)
+            const char *e = getenv("CUFSP_ARNOLDI_CTA_STATES");
+            return e ? std::max<int64_t>(32, atoll(e)) : (int64_t)256;
+        }();
         const int sms = device_info().sm_count;
-        const int64_t want = std::max<int64_t>(1, std::min<int64_t>(sms, (n + 255) / 256));
+        const int64_t want = std::max<int64_t>(1, std::min<int64_t>(sms, (n + min_states - 1) / min_states));
         const int64_t chunk = (n + want - 1) / want;
         const int64_t grid = (n + chunk - 1) / chunk;
         const size_t smem = sizeof(double) * ((size_t)chunk + (size_t)std::max(1, m) * grid);
