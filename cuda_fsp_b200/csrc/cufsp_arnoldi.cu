@@ -508,8 +508,12 @@ cufsp_status parnoldi_run(PArnoldi **ppa, cufsp_mat *A, const std::vector<double
         const size_t smem = sizeof(double) * ((size_t)chunk + (size_t)std::max(1, m) * grid);
         if (smem > (size_t)device_info().max_smem_optin - sizeof(PSmem) - 1024)
             return set_error(CUFSP_ERR_UNSUPPORTED, "persistent Arnoldi: vector slice exceeds shared memory");
-        CUFSP_CUDA_TRY(cudaFuncSetAttribute((const void *)k_arnoldi_persistent,
-                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        // The attribute is process-wide: set it once to the most any driver may ask for, so that
+        // drivers of different sizes on different host threads never undercut each other.
+        static const cudaError_t attr = cudaFuncSetAttribute(
+            (const void *)k_arnoldi_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            device_info().max_smem_optin - (int)sizeof(PSmem) - 1024);
+        CUFSP_CUDA_TRY(attr);
         int per_sm = 0;
         CUFSP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k_arnoldi_persistent,
                                                                      kPThreads, smem));
