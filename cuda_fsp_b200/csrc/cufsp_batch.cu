@@ -305,7 +305,8 @@ cufsp_status autotune(cufsp_batch *B, double t_final, const double *p, cudaStrea
         B->threads = sh.threads;
         B->minb = sh.minb;
     } else {
-        const Shape cands[] = {{8, 256, 1}, {16, 256, 1}, {8, 512, 1}, {16, 512, 1}, {8, 256, 2}, {16, 256, 2}};
+        const Shape cands[] = {{8, 256, 1}, {16, 256, 1}, {4, 512, 1}, {8, 512, 1},
+                               {16, 512, 1}, {8, 256, 2}, {16, 256, 2}};
         const int64_t total = B->offsets.back();
         if (!B->d_scratch) CUFSP_CUDA_TRY(cudaMalloc(&B->d_scratch, sizeof(double) * (size_t)total));
         double best = 1e300;
