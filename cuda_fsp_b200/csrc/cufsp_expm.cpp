@@ -18,76 +18,96 @@ namespace cufsp {
 
 namespace {
 
-// C = A * B, column-major, four columns of C per pass over A (the inner loop is unit-stride).
-// Cloned for AVX-512, AVX2 and baseline x86-64; the loader picks the widest the host supports.
-__attribute__((target_clones("avx512f", "avx2", "default"))) void matmul(int k, const double *__restrict A,
+// The exponential works on kp x kp matrices, kp = k rounded up to a multiple of 8, with A embedded
+// as the leading block of block-diag(A, 0): exp of that is block-diag(exp A, I), so the padding
+// changes nothing in the leading block and every column is a whole number of 8-double vectors.
+typedef double v8 __attribute__((vector_size(64), aligned(8)));
+
+inline v8 ld8(const double *p) {
+    v8 v;
+    std::memcpy(&v, p, sizeof(v));
+    return v;
+}
+inline void st8(double *p, v8 v) { std::memcpy(p, &v, sizeof(v)); }
+
+// C = A B, column-major kp x kp (kp % 8 == 0): four columns of C kept in vector registers while one
+// column of A streams past.  Cloned for AVX-512, AVX2 and baseline x86-64; the loader picks the
+// widest the host supports.
+__attribute__((target_clones("avx512f", "avx2", "default"))) void matmul(int kp, const double *__restrict A,
                                                                          const double *__restrict B,
                                                                          double *__restrict C) {
-    int j = 0;
-    for (; j + 4 <= k; j += 4) {
-        double *__restrict c0 = C + (size_t)j * k;
-        double *__restrict c1 = c0 + k;
-        double *__restrict c2 = c1 + k;
-        double *__restrict c3 = c2 + k;
-        for (int i = 0; i < k; ++i) c0[i] = c1[i] = c2[i] = c3[i] = 0.0;
-        for (int l = 0; l < k; ++l) {
-            const double b0 = B[l + (size_t)j * k], b1 = B[l + (size_t)(j + 1) * k];
-            const double b2 = B[l + (size_t)(j + 2) * k], b3 = B[l + (size_t)(j + 3) * k];
-            const double *__restrict al = A + (size_t)l * k;
-            for (int i = 0; i < k; ++i) {
-                const double a = al[i];
-                c0[i] += a * b0;
-                c1[i] += a * b1;
-                c2[i] += a * b2;
-                c3[i] += a * b3;
+    for (int j = 0; j < kp; j += 4) {
+        const double *b0 = B + (size_t)j * kp, *b1 = b0 + kp, *b2 = b1 + kp, *b3 = b2 + kp;
+        for (int r = 0; r < kp; r += 8) {
+            v8 c0 = {0, 0, 0, 0, 0, 0, 0, 0}, c1 = c0, c2 = c0, c3 = c0;
+            for (int l = 0; l < kp; ++l) {
+                const v8 a = ld8(A + (size_t)l * kp + r);
+                c0 += a * b0[l];
+                c1 += a * b1[l];
+                c2 += a * b2[l];
+                c3 += a * b3[l];
             }
-        }
-    }
-    for (; j < k; ++j) {
-        double *__restrict cj = C + (size_t)j * k;
-        for (int i = 0; i < k; ++i) cj[i] = 0.0;
-        for (int l = 0; l < k; ++l) {
-            const double b = B[l + (size_t)j * k];
-            const double *__restrict al = A + (size_t)l * k;
-            for (int i = 0; i < k; ++i) cj[i] += al[i] * b;
+            st8(C + (size_t)j * kp + r, c0);
+            st8(C + (size_t)(j + 1) * kp + r, c1);
+            st8(C + (size_t)(j + 2) * kp + r, c2);
+            st8(C + (size_t)(j + 3) * kp + r, c3);
         }
     }
 }
 
-// Solve P X = Q in place (X overwrites Q) by LU with partial pivoting.  Returns false if P is
-// singular to working precision.
-bool lu_solve(int k, std::vector<double> &P, std::vector<double> &Q) {
-    std::vector<int> piv(k);
-    for (int c = 0; c < k; ++c) {
+// X = P^{-1} Q by LU with partial pivoting.  P and Q are column-major kp x kp on entry; they are
+// transposed into row-major work arrays so that every elimination and substitution step is a
+// contiguous row operation.  X (column-major) overwrites Q.  False if P is singular.
+__attribute__((target_clones("avx512f", "avx2", "default"))) bool lu_solve(int kp, const double *__restrict Pc,
+                                                                           double *__restrict Qc, double *__restrict P,
+                                                                           double *__restrict Q) {
+    for (int i = 0; i < kp; ++i)
+        for (int j = 0; j < kp; ++j) {
+            P[(size_t)i * kp + j] = Pc[i + (size_t)j * kp];
+            Q[(size_t)i * kp + j] = Qc[i + (size_t)j * kp];
+        }
+    for (int c = 0; c < kp; ++c) {
         int p = c;
-        double best = std::fabs(P[c + (size_t)c * k]);
-        for (int i = c + 1; i < k; ++i) {
-            const double v = std::fabs(P[i + (size_t)c * k]);
-            if (v > best) { best = v; p = i; }
+        double best = std::fabs(P[(size_t)c * kp + c]);
+        for (int i = c + 1; i < kp; ++i) {
+            const double v = std::fabs(P[(size_t)i * kp + c]);
+            if (v > best) {
+                best = v;
+                p = i;
+            }
         }
         if (best == 0.0) return false;
-        piv[c] = p;
         if (p != c)
-            for (int j = 0; j < k; ++j) std::swap(P[c + (size_t)j * k], P[p + (size_t)j * k]);
-        const double inv = 1.0 / P[c + (size_t)c * k];
-        for (int i = c + 1; i < k; ++i) P[i + (size_t)c * k] *= inv;
-        for (int j = c + 1; j < k; ++j) {
-            const double u = P[c + (size_t)j * k];
+            for (int j = 0; j < kp; ++j) {
+                std::swap(P[(size_t)c * kp + j], P[(size_t)p * kp + j]);
+                std::swap(Q[(size_t)c * kp + j], Q[(size_t)p * kp + j]);
+            }
+        const double inv = 1.0 / P[(size_t)c * kp + c];
+        const double *__restrict pc = P + (size_t)c * kp;
+        const double *__restrict qc = Q + (size_t)c * kp;
+        for (int i = c + 1; i < kp; ++i) {
+            double *__restrict pi = P + (size_t)i * kp;
+            double *__restrict qi = Q + (size_t)i * kp;
+            const double l = pi[c] * inv;
+            if (l == 0.0) continue;
+            for (int j = c + 1; j < kp; ++j) pi[j] -= l * pc[j];
+            for (int j = 0; j < kp; ++j) qi[j] -= l * qc[j];
+        }
+    }
+    for (int c = kp - 1; c >= 0; --c) {  // back substitution, whole rows of Q at a time
+        double *__restrict qc = Q + (size_t)c * kp;
+        const double *__restrict pc = P + (size_t)c * kp;
+        for (int i = c + 1; i < kp; ++i) {
+            const double u = pc[i];
             if (u == 0.0) continue;
-            for (int i = c + 1; i < k; ++i) P[i + (size_t)j * k] -= P[i + (size_t)c * k] * u;
+            const double *__restrict qi = Q + (size_t)i * kp;
+            for (int j = 0; j < kp; ++j) qc[j] -= u * qi[j];
         }
+        const double inv = 1.0 / pc[c];
+        for (int j = 0; j < kp; ++j) qc[j] *= inv;
     }
-    for (int j = 0; j < k; ++j) {
-        double *q = Q.data() + (size_t)j * k;
-        for (int c = 0; c < k; ++c)
-            if (piv[c] != c) std::swap(q[c], q[piv[c]]);
-        for (int c = 0; c < k; ++c)  // unit lower
-            for (int i = c + 1; i < k; ++i) q[i] -= P[i + (size_t)c * k] * q[c];
-        for (int c = k - 1; c >= 0; --c) {  // upper
-            q[c] /= P[c + (size_t)c * k];
-            for (int i = 0; i < c; ++i) q[i] -= P[i + (size_t)c * k] * q[c];
-        }
-    }
+    for (int i = 0; i < kp; ++i)
+        for (int j = 0; j < kp; ++j) Qc[i + (size_t)j * kp] = Q[(size_t)i * kp + j];
     return true;
 }
 
@@ -100,7 +120,6 @@ cufsp_status expm_pade13(int k, const double *A, double *F) {
     c[0] = 1.0;
     for (int j = 0; j < m; ++j) c[j + 1] = c[j] * (double)(m - j) / ((double)(j + 1) * (double)(2 * m - j));
 
-    const size_t sz = (size_t)k * k;
     double norm1 = 0.0;
     for (int j = 0; j < k; ++j) {
         double s = 0.0;
@@ -113,35 +132,43 @@ cufsp_status expm_pade13(int k, const double *A, double *F) {
     if (norm1 > theta13) sq = (int)std::ceil(std::log2(norm1 / theta13));
     const double scale = std::ldexp(1.0, -sq);
 
-    std::vector<double> B(sz), B2(sz), B4(sz), B6(sz), T(sz), U(sz), V(sz), W(sz);
-    for (size_t i = 0; i < sz; ++i) B[i] = A[i] * scale;
-    matmul(k, B.data(), B.data(), B2.data());
-    matmul(k, B2.data(), B2.data(), B4.data());
-    matmul(k, B4.data(), B2.data(), B6.data());
+    const int kp = (k + 7) & ~7;
+    const size_t sz = (size_t)kp * kp;
+    thread_local std::vector<double> work;  // 12 kp x kp matrices, reused across calls
+    if (work.size() < 12 * sz) work.assign(12 * sz, 0.0);
+    double *B = work.data(), *B2 = B + sz, *B4 = B2 + sz, *B6 = B4 + sz, *T = B6 + sz, *U = T + sz, *V = U + sz,
+           *W = V + sz, *P = W + sz, *Q = P + sz, *Pr = Q + sz, *Qr = Pr + sz;
+    std::memset(B, 0, sizeof(double) * sz);
+    for (int j = 0; j < k; ++j)
+        for (int i = 0; i < k; ++i) B[i + (size_t)j * kp] = A[i + (size_t)j * k] * scale;
+    matmul(kp, B, B, B2);
+    matmul(kp, B2, B2, B4);
+    matmul(kp, B4, B2, B6);
     // odd part U = B (B6 (c13 B6 + c11 B4 + c9 B2) + c7 B6 + c5 B4 + c3 B2 + c1 I)
     for (size_t i = 0; i < sz; ++i) T[i] = c[13] * B6[i] + c[11] * B4[i] + c[9] * B2[i];
-    matmul(k, B6.data(), T.data(), W.data());
+    matmul(kp, B6, T, W);
     for (size_t i = 0; i < sz; ++i) W[i] += c[7] * B6[i] + c[5] * B4[i] + c[3] * B2[i];
-    for (int i = 0; i < k; ++i) W[i + (size_t)i * k] += c[1];
-    matmul(k, B.data(), W.data(), U.data());
+    for (int i = 0; i < kp; ++i) W[i + (size_t)i * kp] += c[1];
+    matmul(kp, B, W, U);
     // even part V = B6 (c12 B6 + c10 B4 + c8 B2) + c6 B6 + c4 B4 + c2 B2 + c0 I
     for (size_t i = 0; i < sz; ++i) T[i] = c[12] * B6[i] + c[10] * B4[i] + c[8] * B2[i];
-    matmul(k, B6.data(), T.data(), V.data());
+    matmul(kp, B6, T, V);
     for (size_t i = 0; i < sz; ++i) V[i] += c[6] * B6[i] + c[4] * B4[i] + c[2] * B2[i];
-    for (int i = 0; i < k; ++i) V[i + (size_t)i * k] += c[0];
+    for (int i = 0; i < kp; ++i) V[i + (size_t)i * kp] += c[0];
     // (V - U) R = (V + U)
-    std::vector<double> P(sz), Q(sz);
     for (size_t i = 0; i < sz; ++i) {
         P[i] = V[i] - U[i];
         Q[i] = V[i] + U[i];
     }
-    if (!lu_solve(k, P, Q)) return set_error(CUFSP_ERR_NONFINITE, "expm: singular Pade denominator");
+    if (!lu_solve(kp, P, Q, Pr, Qr)) return set_error(CUFSP_ERR_NONFINITE, "expm: singular Pade denominator");
+    double *R = Q, *S = T;
     for (int i = 0; i < sq; ++i) {
-        matmul(k, Q.data(), Q.data(), T.data());
-        Q.swap(T);
+        matmul(kp, R, R, S);
+        std::swap(R, S);
     }
-    std::memcpy(F, Q.data(), sizeof(double) * sz);
-    for (size_t i = 0; i < sz; ++i)
+    for (int j = 0; j < k; ++j)
+        for (int i = 0; i < k; ++i) F[i + (size_t)j * k] = R[i + (size_t)j * kp];
+    for (size_t i = 0; i < (size_t)k * k; ++i)
         if (!std::isfinite(F[i])) return set_error(CUFSP_ERR_NONFINITE, "expm: result holds NaN/Inf");
     return CUFSP_SUCCESS;
 }
