@@ -66,7 +66,8 @@ def test_reference_mass_conservation_case(cuda):
         assert abs(1.0 - w.sum()) <= 1e-10
         assert np.abs(w - truth).sum() <= budget
     w_full, _ = run_gpu(m, T, MatrixFormat.KRONECKER, m=40, tol=1e-12)
-    assert np.abs(w_full - truth).sum() <= 1e-9
+    # the same budget argument for the tight solve: its own delta*tol*T plus the truth's
+    assert np.abs(w_full - truth).sum() <= 1.2 * (1e-12 + 1e-13) * T
 
 
 def test_callback_matvec_equals_generator_path(cuda):
