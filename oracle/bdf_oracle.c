@@ -84,10 +84,25 @@ static int bdf_apply(const bdf_op *A, double t, double alpha, const double *x, i
     return ORC_OK;
 }
 
+/* Weighted dot product in a fixed summation order whatever the thread count (64 fixed blocks, then
+ * the block sums in order), so that the integrator's decisions do not change from run to run. */
 static double wdot(int64_t n, const double *x, const double *y, const double *w) {
+    enum { NB = 64 };
+    double part[NB];
+    if (n < 8192) {
+        double s = 0.0;
+        for (int64_t i = 0; i < n; ++i) s += x[i] * y[i] * w[i] * w[i];
+        return s;
+    }
+#pragma omp parallel for schedule(static)
+    for (int b = 0; b < NB; ++b) {
+        const int64_t lo = n * b / NB, hi = n * (b + 1) / NB;
+        double s = 0.0;
+        for (int64_t i = lo; i < hi; ++i) s += x[i] * y[i] * w[i] * w[i];
+        part[b] = s;
+    }
     double s = 0.0;
-#pragma omp parallel for reduction(+ : s) schedule(static)
-    for (int64_t i = 0; i < n; ++i) s += x[i] * y[i] * w[i] * w[i];
+    for (int b = 0; b < NB; ++b) s += part[b];
     return s;
 }
 

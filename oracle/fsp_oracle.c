@@ -368,12 +368,30 @@ static void orc_op_apply(const orc_op *A, const double *x, double *y) {
     orc_spmv(A->n, A->nr, A->rowptr, A->col, A->val, A->coefs, x, 0.0, y);
 }
 
-static double orc_nrm2(int64_t n, const double *x) {
+/* x . y in a fixed summation order whatever the thread count: 64 fixed blocks summed in parallel,
+ * then the block sums in order (an OpenMP reduction combines per-thread sums in an unspecified
+ * order, which made borderline breakdown decisions change from run to run). */
+static double orc_dot(int64_t n, const double *x, const double *y) {
+    enum { NB = 64 };
+    double part[NB];
+    if (n < 8192) {
+        double s = 0.0;
+        for (int64_t i = 0; i < n; ++i) s += x[i] * y[i];
+        return s;
+    }
+#pragma omp parallel for schedule(static)
+    for (int b = 0; b < NB; ++b) {
+        const int64_t lo = n * b / NB, hi = n * (b + 1) / NB;
+        double s = 0.0;
+        for (int64_t i = lo; i < hi; ++i) s += x[i] * y[i];
+        part[b] = s;
+    }
     double s = 0.0;
-#pragma omp parallel for reduction(+ : s) schedule(static)
-    for (int64_t i = 0; i < n; ++i) s += x[i] * x[i];
-    return sqrt(s);
+    for (int b = 0; b < NB; ++b) s += part[b];
+    return s;
 }
+
+static double orc_nrm2(int64_t n, const double *x) { return sqrt(orc_dot(n, x, x)); }
 
 typedef struct {
     int64_t n_steps, n_reject, n_matvec;
@@ -427,9 +445,7 @@ int orc_expv(int64_t n, int nr, const int *rowptr, const int *col, const double 
             /* h = V[istart..j]^T w (first gemv), then w -= V h (second gemv) */
             for (int k = istart; k <= j; ++k) {
                 const double *vk = Vb + (int64_t)k * n;
-                double s = 0.0;
-#pragma omp parallel for reduction(+ : s) schedule(static)
-                for (int64_t i = 0; i < n; ++i) s += vk[i] * w[i];
+                const double s = orc_dot(n, vk, w);
                 h[k] = s;
                 H[k + j * mp2] = s;
             }
