@@ -352,15 +352,15 @@ struct PArnoldi {
 void parnoldi_destroy(PArnoldi *pa) {
     if (!pa) return;
     for (auto &t : pa->terms)
-        if (t.d_coef) cudaFree(t.d_coef);
-    if (pa->d_nu) cudaFree(pa->d_nu);
-    if (pa->d_tables) cudaFree(pa->d_tables);
-    if (pa->d_c) cudaFree(pa->d_c);
-    if (pa->d_rterm) cudaFree(pa->d_rterm);
-    if (pa->d_d) cudaFree(pa->d_d);
-    if (pa->d_props) cudaFree(pa->d_props);
-    if (pa->d_part) cudaFree(pa->d_part);
-    if (pa->d_bar) cudaFree(pa->d_bar);
+        cache_free(t.d_coef);
+    cache_free(pa->d_nu);
+    cache_free(pa->d_tables);
+    cache_free(pa->d_c);
+    cache_free(pa->d_rterm);
+    cache_free(pa->d_d);
+    cache_free(pa->d_props);
+    cache_free(pa->d_part);
+    cache_free(pa->d_bar);
     delete pa;
 }
 
@@ -425,14 +425,14 @@ cufsp_status build_terms(PArnoldi *pa, cufsp_mat *A, const std::vector<double> &
     shifts.push_back(0);
     // model data on the device (once per generator)
     if (!pa->d_nu) {
-        CUFSP_CUDA_TRY(cudaMalloc(&pa->d_nu, sizeof(int) * (size_t)nr * ns));
+        CUFSP_CUDA_TRY(cache_alloc((void **)&pa->d_nu, sizeof(int) * (size_t)nr * ns));
         CUFSP_CUDA_TRY(cudaMemcpy(pa->d_nu, m.nu.data(), sizeof(int) * (size_t)nr * ns, cudaMemcpyHostToDevice));
-        CUFSP_CUDA_TRY(cudaMalloc(&pa->d_c, sizeof(double) * nr));
-        CUFSP_CUDA_TRY(cudaMalloc(&pa->d_rterm, sizeof(int) * nr * 2));
-        CUFSP_CUDA_TRY(cudaMalloc(&pa->d_d, sizeof(int64_t) * nr));
+        CUFSP_CUDA_TRY(cache_alloc((void **)&pa->d_c, sizeof(double) * nr));
+        CUFSP_CUDA_TRY(cache_alloc((void **)&pa->d_rterm, sizeof(int) * nr * 2));
+        CUFSP_CUDA_TRY(cache_alloc((void **)&pa->d_d, sizeof(int64_t) * nr));
         CUFSP_CUDA_TRY(cudaMemcpy(pa->d_d, d.data(), sizeof(int64_t) * nr, cudaMemcpyHostToDevice));
         if (A->format == CUFSP_FORMAT_KRONECKER) {
-            CUFSP_CUDA_TRY(cudaMalloc(&pa->d_tables, sizeof(double) * m.tables.size()));
+            CUFSP_CUDA_TRY(cache_alloc((void **)&pa->d_tables, sizeof(double) * m.tables.size()));
             CUFSP_CUDA_TRY(cudaMemcpy(pa->d_tables, m.tables.data(), sizeof(double) * m.tables.size(),
                                       cudaMemcpyHostToDevice));
         }
@@ -452,7 +452,7 @@ cufsp_status build_terms(PArnoldi *pa, cufsp_mat *A, const std::vector<double> &
     if (A->format == CUFSP_FORMAT_KRONECKER) {
         b.tables = pa->d_tables;
     } else {
-        if (!pa->d_props) CUFSP_CUDA_TRY(cudaMalloc(&pa->d_props, sizeof(double) * (size_t)nr * n));
+        if (!pa->d_props) CUFSP_CUDA_TRY(cache_alloc((void **)&pa->d_props, sizeof(double) * (size_t)nr * n));
         cufsp_status s = sparse_export(A->sparse, pa->d_props, st);
         if (s != CUFSP_SUCCESS) return s;
         b.props = pa->d_props;
@@ -466,9 +466,9 @@ cufsp_status build_terms(PArnoldi *pa, cufsp_mat *A, const std::vector<double> &
     b.rterm = d_rt;
     b.d = pa->d_d;
     if (!tm.d_coef || tm.T < T) {
-        if (tm.d_coef) cudaFree(tm.d_coef);
+        cache_free(tm.d_coef);
         tm.d_coef = nullptr;
-        CUFSP_CUDA_TRY(cudaMalloc(&tm.d_coef, sizeof(double) * (size_t)T * n));
+        CUFSP_CUDA_TRY(cache_alloc((void **)&tm.d_coef, sizeof(double) * (size_t)T * n));
     }
     b.coef = tm.d_coef;
     const int grid = stream_grid(n, 1, device_info().sm_count * 8);
@@ -521,8 +521,8 @@ cufsp_status parnoldi_run(PArnoldi **ppa, cufsp_mat *A, const std::vector<double
         pa->grid = (int)grid;
         pa->chunk = chunk;
         pa->smem = smem;
-        CUFSP_CUDA_TRY(cudaMalloc(&pa->d_part, sizeof(double) * 2 * (size_t)pa->grid * kKMax));
-        CUFSP_CUDA_TRY(cudaMalloc(&pa->d_bar, sizeof(unsigned)));
+        CUFSP_CUDA_TRY(cache_alloc((void **)&pa->d_part, sizeof(double) * 2 * (size_t)pa->grid * kKMax));
+        CUFSP_CUDA_TRY(cache_alloc((void **)&pa->d_bar, sizeof(unsigned)));
     }
     PArgs a;
     std::memset(&a, 0, sizeof(a));

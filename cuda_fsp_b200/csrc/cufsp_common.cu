@@ -3,7 +3,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
+#include <unordered_map>
 
 #include "cufsp_internal.h"
 #include "cufsp_reduce.cuh"
@@ -62,19 +64,108 @@ int stream_grid(int64_t n, int elems_per_thread, int max_ctas) {
     return (int)g;
 }
 
+// ---- cached device buffers -------------------------------------------------------------------
+// Krylov drivers are typically created and destroyed once per solve (the reference's usage); with
+// plain cudaMalloc/cudaFree every solve pays the driver's page-table work and an implicit device
+// synchronisation per buffer (2-6 ms per small solve measured).  Their buffers come from this cache
+// instead: a released buffer is kept (after a device synchronisation, since kernels may still use
+// it) and handed to the next request of a similar size on the same device.
+namespace {
+struct CachedBlock {
+    void *p;
+    size_t bytes;
+    int dev;
+};
+struct BufferCache {
+    std::mutex mu;
+    std::multimap<size_t, CachedBlock> idle;  // by size
+    std::unordered_map<void *, CachedBlock> live;
+    size_t idle_bytes = 0;
+};
+BufferCache &buffer_cache() {
+    static BufferCache *c = new BufferCache();  // never destroyed: no CUDA calls at process exit
+    return *c;
+}
+constexpr size_t kCacheCap = (size_t)1 << 30;  // idle bytes kept at most
+}  // namespace
+
+cudaError_t cache_alloc(void **p, size_t bytes) {
+    *p = nullptr;
+    bytes = (std::max<size_t>(bytes, 1) + 255) & ~(size_t)255;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    BufferCache &c = buffer_cache();
+    {
+        std::lock_guard<std::mutex> lk(c.mu);
+        for (auto it = c.idle.lower_bound(bytes); it != c.idle.end() && it->first <= 2 * bytes; ++it) {
+            if (it->second.dev != dev) continue;
+            CachedBlock b = it->second;
+            c.idle.erase(it);
+            c.idle_bytes -= b.bytes;
+            c.live[b.p] = b;
+            *p = b.p;
+            return cudaSuccess;
+        }
+    }
+    e = cudaMalloc(p, bytes);
+    if (e == cudaErrorMemoryAllocation) {  // give the idle buffers of this device back and retry
+        cudaGetLastError();
+        std::lock_guard<std::mutex> lk(c.mu);
+        for (auto it = c.idle.begin(); it != c.idle.end();) {
+            if (it->second.dev == dev) {
+                cudaFree(it->second.p);
+                c.idle_bytes -= it->second.bytes;
+                it = c.idle.erase(it);
+            } else {
+                ++it;
+            }
+        }
+        e = cudaMalloc(p, bytes);
+    }
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(c.mu);
+    c.live[*p] = CachedBlock{*p, bytes, dev};
+    return cudaSuccess;
+}
+
+void cache_free(void *p) {
+    if (!p) return;
+    BufferCache &c = buffer_cache();
+    CachedBlock b;
+    {
+        std::lock_guard<std::mutex> lk(c.mu);
+        auto it = c.live.find(p);
+        if (it == c.live.end()) {
+            cudaFree(p);
+            return;
+        }
+        b = it->second;
+        c.live.erase(it);
+    }
+    cudaDeviceSynchronize();  // work still queued may use the buffer
+    std::lock_guard<std::mutex> lk(c.mu);
+    if (c.idle_bytes + b.bytes > kCacheCap) {
+        cudaFree(b.p);
+        return;
+    }
+    c.idle.emplace(b.bytes, b);
+    c.idle_bytes += b.bytes;
+}
+
 cufsp_status ReduceScratch::init(int ctas, int k) {
     release();
     max_ctas = ctas;
     max_k = k;
-    CUFSP_CUDA_TRY(cudaMalloc(&partials, sizeof(double) * (size_t)ctas * k));
-    CUFSP_CUDA_TRY(cudaMalloc(&counter, sizeof(unsigned int) * 4));
+    CUFSP_CUDA_TRY(cache_alloc((void **)&partials, sizeof(double) * (size_t)ctas * k));
+    CUFSP_CUDA_TRY(cache_alloc((void **)&counter, sizeof(unsigned int) * 4));
     CUFSP_CUDA_TRY(cudaMemset(counter, 0, sizeof(unsigned int) * 4));
     return CUFSP_SUCCESS;
 }
 
 void ReduceScratch::release() {
-    if (partials) cudaFree(partials);
-    if (counter) cudaFree(counter);
+    cache_free(partials);
+    cache_free(counter);
     partials = nullptr;
     counter = nullptr;
 }

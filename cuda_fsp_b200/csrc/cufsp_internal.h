@@ -57,6 +57,11 @@ __host__ __device__ __forceinline__ uint32_t fd_div(uint32_t n, const FastDiv &f
 
 // Reduction scratch shared by the vector kernels of one handle: per-CTA partials and a
 // completion counter for the last-CTA-reduces pattern (deterministic summation order).
+// Device buffers from a per-process cache (cufsp_common.cu): cache_free synchronises the device and
+// keeps the buffer for the next cache_alloc of a similar size on the same device.
+cudaError_t cache_alloc(void **p, size_t bytes);
+void cache_free(void *p);
+
 struct ReduceScratch {
     double *partials = nullptr;  // [max_ctas * max_k]
     unsigned int *counter = nullptr;

@@ -510,8 +510,8 @@ extern "C" cufsp_status cufsp_expv_create(int64_t n, int m, double tol, int iop,
     E->F.resize((size_t)mp2 * mp2);
     E->tH.resize((size_t)mp2 * mp2);
     std::memset(&E->stats, 0, sizeof(E->stats));
-    cudaError_t e = cudaMalloc(&E->W, sizeof(double) * (size_t)n * (size_t)(m + 1));
-    if (e == cudaSuccess) e = cudaMalloc(&E->d_state, E->state_bytes);
+    cudaError_t e = cache_alloc((void **)&E->W, sizeof(double) * (size_t)n * (size_t)(m + 1));
+    if (e == cudaSuccess) e = cache_alloc((void **)&E->d_state, E->state_bytes);
     if (e == cudaSuccess) e = cudaMemset(E->d_state, 0, E->state_bytes);
     if (e != cudaSuccess) {
         cufsp_expv_destroy(E);
@@ -540,8 +540,8 @@ extern "C" cufsp_status cufsp_expv_destroy(cufsp_expv *E) {
     for (auto &g : E->graphs) cudaGraphExecDestroy(g.exec);
     parnoldi_destroy(E->pa);
     if (E->cap_stream) cudaStreamDestroy(E->cap_stream);
-    if (E->W) cudaFree(E->W);
-    if (E->d_state) cudaFree(E->d_state);
+    cache_free(E->W);
+    cache_free(E->d_state);
     E->rs.release();
     delete E;
     return CUFSP_SUCCESS;
