@@ -285,7 +285,7 @@ def expmv_large_secondary(max_steps: int = 400, budget_s: float = 12.0) -> dict:
 
 
 def bdf_secondary() -> dict:
-    """C2: the time-varying gene-expression model (131,072 states, switching rate
+    """BDF leg: the time-varying gene-expression model (131,072 states, switching rate
     k0 sigmoid((t - 5) / 0.5)) from p0 to t = 60 by the device BDF integrator (rtol 1e-8, atol 1e-14;
     the reference's CVODE path).  The oracle's host BDF is timed on the sample [0, 6] (the switch and
     408 of the ~700 steps), with the device solve of the same sample beside it."""
@@ -331,7 +331,7 @@ def cpu_expmv_ms() -> float:
 
 
 def batched_secondary(n_sets: int = 256, sample: int = 4) -> dict:
-    """C4: n_sets parameter sets of the gene-expression model (rates within one decade of nominal,
+    """Batched leg: n_sets parameter sets of the gene-expression model (rates within one decade of nominal,
     mRNA bounds 63..255) solved to t = 30 in one persistent launch; the plain single-instance Krylov
     path is timed on `sample` of the same instances and its results compared (1-norm)."""
     import torch
@@ -372,7 +372,7 @@ def batched_secondary(n_sets: int = 256, sample: int = 4) -> dict:
 
 
 def batched_sharded_secondary(world: int, rank: int, dev, per_rank: int = 256) -> dict | None:
-    """C4 over N GPUs: per_rank * N parameter sets partitioned by state count over the ranks
+    """Batched leg over N GPUs: per_rank * N parameter sets partitioned by state count over the ranks
     (cuda_fsp_b200.batch.solve_sharded, weak scaling), one final gather of the per-instance results;
     time = max over ranks."""
     import torch
@@ -396,7 +396,7 @@ def batched_sharded_secondary(world: int, rank: int, dev, per_rank: int = 256) -
 
 
 def gradient_secondary(n_sets: int = 64, workers: int = 2) -> dict:
-    """C5: d log L / d log theta for the 12 rates of the gene-expression model (131,072 states) from
+    """Gradient leg: d log L / d log theta for the 12 rates of the gene-expression model (131,072 states) from
     1,000 seeded-SSA cells at 8 log-spaced times in [1, 60], (n, c) histograms marginalised over the
     gene states, for n_sets parameter sets (rates within half a decade of nominal) at once
     (cufsp_likelihood_grad_batched: `workers` concurrent adjoint solves; at this size each solve's

@@ -51,7 +51,7 @@ def test_adjoint_matches_forward_sensitivity(cuda, case):
 
 
 def test_adjoint_matches_central_differences(cuda):
-    """C5 shape: 1,000 SSA cells at 8 log-spaced times in [1, 60], (n, c) histograms marginalised
+    """The gradient benchmark's data shape: 1,000 SSA cells at 8 log-spaced times in [1, 60], (n, c) histograms marginalised
     over the gene states; d log L / d log theta for all 12 rates against central differences
     (h = 1e-5) of the host log-likelihood."""
     m = models.gene_expression((1, 1, 1, 31, 31), time_varying=False)
