@@ -284,6 +284,36 @@ def expmv_large_secondary(max_steps: int = 400, budget_s: float = 12.0) -> dict:
             "mass": round(v.sum().item(), 12)}
 
 
+def sparse_secondary(steps: int = 200) -> dict:
+    """The sparse-format generator action (CSR/HYB: reaction-major propensity table a_r(x_i)) on the
+    255^3 workload, y += A x over 2 rotating (x, y) pairs (537 MB > L2), CUDA events.  Algorithmic
+    bytes: x read, y read and written, and the nr-row table read: (24 + 8 nr) B/state."""
+    import torch
+    from cuda_fsp_b200 import FSPMat, MatrixFormat, models
+    m = models.mass_action_3()
+    n = m.n_states
+    A = FSPMat.from_model(m, MatrixFormat.HYB)
+    g = torch.Generator(device="cuda").manual_seed(5)
+    xs = [torch.rand(n, dtype=torch.float64, device="cuda", generator=g) for _ in range(2)]
+    ys = [torch.zeros(n, dtype=torch.float64, device="cuda") for _ in range(2)]
+    for i in range(4):
+        A.action(0.0, xs[i % 2], ys[i % 2])
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for i in range(steps):
+        A.action(0.0, xs[i % 2], ys[i % 2])
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    bps = 24 + 8 * m.nr
+    gbs = bps * n / (ms * 1e-3) / 1e9
+    peak, _ = measured_peak_hbm()
+    return {"metric": "sparse-format matvec GB/s", "workload": "mass_action_3 255^3, HYB (propensity table), y += A x",
+            "value": round(gbs, 1), "us_per_action": round(ms * 1e3, 2), "bytes_per_state": bps,
+            "frac_of_hbm_peak": round(gbs / peak, 4), "kernel": A.describe()}
+
+
 def bdf_secondary() -> dict:
     """BDF leg: the time-varying gene-expression model (131,072 states, switching rate
     k0 sigmoid((t - 5) / 0.5)) from p0 to t = 60 by the device BDF integrator (rtol 1e-8, atol 1e-14;
@@ -523,7 +553,8 @@ def run_ours(args):
     elif rank == 0:
         secondary = expmv_secondary()
         secondary["cpu_oracle_ms_per_solve"] = round(cpu_expmv_ms(), 1)
-        secondary = [secondary, bdf_secondary(), expmv_large_secondary(), batched_secondary(), gradient_secondary()]
+        secondary = [secondary, sparse_secondary(), bdf_secondary(), expmv_large_secondary(), batched_secondary(),
+                     gradient_secondary()]
     cpu = cpu_oracle_gbs(max(3, min(args.steps, 20)), 1) if (rank == 0 and world == 1) else None
     peak, peak_kind = measured_peak_hbm()
     if rank == 0:
