@@ -21,14 +21,17 @@ namespace {
 // The exponential works on kp x kp matrices, kp = k rounded up to a multiple of 8, with A embedded
 // as the leading block of block-diag(A, 0): exp of that is block-diag(exp A, I), so the padding
 // changes nothing in the leading block and every column is a whole number of 8-double vectors.
+// (GCC notes that a 64-byte vector changes the calling convention without AVX-512; the helpers below
+// have internal linkage and are always inlined, so no call ever passes one.)
+#pragma GCC diagnostic ignored "-Wpsabi"
 typedef double v8 __attribute__((vector_size(64), aligned(8)));
 
-inline v8 ld8(const double *p) {
+__attribute__((always_inline)) inline v8 ld8(const double *p) {
     v8 v;
     std::memcpy(&v, p, sizeof(v));
     return v;
 }
-inline void st8(double *p, v8 v) { std::memcpy(p, &v, sizeof(v)); }
+__attribute__((always_inline)) inline void st8(double *p, v8 v) { std::memcpy(p, &v, sizeof(v)); }
 
 // C = A B, column-major kp x kp (kp % 8 == 0): four columns of C kept in vector registers while one
 // column of A streams past.  Cloned for AVX-512, AVX2 and baseline x86-64; the loader picks the
