@@ -176,6 +176,7 @@ SIGNATURES = {
     "cufsp_batch_solve": [_P, C.c_double, _P, _P, C.POINTER(BatchStat)],
     "cufsp_batch_describe": [_P, C.c_char_p, C.c_size_t],
     "cufsp_vec_sum_noalloc": [C.c_int64, _P, _P, _P],
+    "cufsp_cache_trim": [C.POINTER(C.c_size_t)],
 }
 _RESTYPE = {"cufsp_status_string": C.c_char_p, "cufsp_last_error": C.c_char_p}
 

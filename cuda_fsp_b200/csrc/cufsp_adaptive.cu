@@ -113,8 +113,8 @@ cufsp_status build_box(cufsp_adaptive *S) {
     if (s == CUFSP_SUCCESS) s = cufsp_expv_create(S->n, S->m, S->kry_tol, 0, 2, 1.0, &S->E);
     if (s == CUFSP_SUCCESS) s = cufsp_expv_bind_mat_coefs(S->E, S->A, S->coefs.data());
     if (s != CUFSP_SUCCESS) return s;
-    if (cudaMalloc(&S->p, sizeof(double) * S->n) != cudaSuccess ||
-        cudaMalloc(&S->p_prev, sizeof(double) * S->n) != cudaSuccess) {
+    if (dev_malloc(&S->p, sizeof(double) * S->n) != cudaSuccess ||
+        dev_malloc(&S->p_prev, sizeof(double) * S->n) != cudaSuccess) {
         cudaGetLastError();
         return set_error(CUFSP_ERR_ALLOC, "adaptive FSP: vector allocation failed");
     }
@@ -163,7 +163,7 @@ cufsp_status expand(cufsp_adaptive *S, const double *v, cudaStream_t st, bool *g
     const int64_t n_old = S->n;
     std::vector<int> old_dims(ns);
     for (int s = 0; s < ns; ++s) old_dims[s] = S->bounds[s] + 1;
-    CUFSP_CUDA_TRY(cudaMalloc(&old, sizeof(double) * n_old));
+    CUFSP_CUDA_TRY(dev_malloc(&old, sizeof(double) * n_old));
     CUFSP_CUDA_TRY(cudaMemcpyAsync(old, S->p_prev, sizeof(double) * n_old, cudaMemcpyDeviceToDevice, st));
     CUFSP_CUDA_TRY(cudaStreamSynchronize(st));
     release_box(S);
@@ -233,7 +233,7 @@ extern "C" cufsp_status cufsp_adaptive_create(const cufsp_model_desc *desc, cons
     S->m = m;
     cufsp_status s = build_box(S);
     if (s == CUFSP_SUCCESS) s = S->rs.init(device_info().sm_count * 4, CUFSP_MAX_SPECIES);
-    if (s == CUFSP_SUCCESS && cudaMalloc(&S->d_red, sizeof(double) * CUFSP_MAX_SPECIES) != cudaSuccess)
+    if (s == CUFSP_SUCCESS && dev_malloc(&S->d_red, sizeof(double) * CUFSP_MAX_SPECIES) != cudaSuccess)
         s = set_error(CUFSP_ERR_ALLOC, "cufsp_adaptive_create: cudaMalloc");
     if (s != CUFSP_SUCCESS) {
         cufsp_adaptive_destroy(S);

@@ -172,14 +172,18 @@ struct Checkpoint {
     double tau;
 };
 
+// Work buffers of one gradient, from the buffer cache; all their uses are ordered on `st`, so their
+// release waits for nothing on other streams (a concurrent gradient on another stream keeps running).
 struct AdjWork {
+    cudaStream_t st;
     std::vector<double *> bufs;
+    explicit AdjWork(cudaStream_t s) : st(s) {}
     ~AdjWork() {
-        for (double *b : bufs) cudaFree(b);
+        for (double *b : bufs) cache_free(b, st);
     }
     double *alloc(size_t n) {
         double *p = nullptr;
-        if (cudaMalloc(&p, sizeof(double) * n) != cudaSuccess) {
+        if (cache_alloc((void **)&p, sizeof(double) * n) != cudaSuccess) {
             cudaGetLastError();
             return nullptr;
         }
@@ -227,7 +231,7 @@ extern "C" cufsp_status cufsp_likelihood_grad(cufsp_mat *A, const double *coefs,
     if (s != CUFSP_SUCCESS) return s;
     expv_set_transpose(eb.E, true);
 
-    AdjWork wk;
+    AdjWork wk(st);
     double *p = wk.alloc(n), *lam = wk.alloc(n), *lam_b = wk.alloc(n), *pf = wk.alloc(n);
     double *g = wk.alloc((size_t)n * n_times);
     double *uh = wk.alloc((size_t)n * (m + 1));
@@ -237,8 +241,9 @@ extern "C" cufsp_status cufsp_likelihood_grad(cufsp_mat *A, const double *coefs,
         return set_error(CUFSP_ERR_ALLOC, "cufsp_likelihood_grad: device allocation failed");
     struct RsGuard {
         ReduceScratch &r;
-        ~RsGuard() { r.release(); }
-    } rsg{rs};
+        cudaStream_t st;
+        ~RsGuard() { r.release(st); }
+    } rsg{rs, st};
     const int red_grid = stream_grid(n, 4, device_info().sm_count * 4);
     s = rs.init(red_grid, 32);
     if (s != CUFSP_SUCCESS) return s;

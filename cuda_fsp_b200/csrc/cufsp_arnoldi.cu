@@ -24,6 +24,8 @@
 #include <cstring>
 #include <map>
 
+#include <mutex>
+
 #include "cufsp_internal.h"
 
 namespace cufsp {
@@ -349,19 +351,29 @@ struct PArnoldi {
     size_t smem = 0;
 };
 
-void parnoldi_destroy(PArnoldi *pa) {
+namespace {
+template <class Free>
+void parnoldi_release(PArnoldi *pa, Free release) {
     if (!pa) return;
-    for (auto &t : pa->terms)
-        cache_free(t.d_coef);
-    cache_free(pa->d_nu);
-    cache_free(pa->d_tables);
-    cache_free(pa->d_c);
-    cache_free(pa->d_rterm);
-    cache_free(pa->d_d);
-    cache_free(pa->d_props);
-    cache_free(pa->d_part);
-    cache_free(pa->d_bar);
+    for (auto &t : pa->terms) release(t.d_coef);
+    release(pa->d_nu);
+    release(pa->d_tables);
+    release(pa->d_c);
+    release(pa->d_rterm);
+    release(pa->d_d);
+    release(pa->d_props);
+    release(pa->d_part);
+    release(pa->d_bar);
     delete pa;
+}
+}  // namespace
+
+void parnoldi_destroy(PArnoldi *pa) {
+    parnoldi_release(pa, [](void *p) { cache_free(p); });
+}
+
+void parnoldi_destroy(PArnoldi *pa, cudaStream_t last_use) {
+    parnoldi_release(pa, [last_use](void *p) { cache_free(p, last_use); });
 }
 
 void parnoldi_thread_disable(bool off) { tl_disabled = off; }
@@ -485,6 +497,26 @@ cufsp_status build_terms(PArnoldi *pa, cufsp_mat *A, const std::vector<double> &
 
 }  // namespace
 
+namespace {
+cudaError_t persistent_smem_attribute() {
+    constexpr int kMaxDevices = 64;
+    static std::mutex mu;
+    static bool done[kMaxDevices] = {};
+    static cudaError_t result[kMaxDevices] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!done[dev]) {
+        result[dev] = cudaFuncSetAttribute((const void *)k_arnoldi_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           device_info().max_smem_optin - (int)sizeof(PSmem) - 1024);
+        done[dev] = true;
+    }
+    return result[dev];
+}
+}  // namespace
+
 cufsp_status parnoldi_run(PArnoldi **ppa, cufsp_mat *A, const std::vector<double> &coefs, bool transpose,
                           int64_t n, const double *v, double *W, double *H, double *rho, double *gam, double *beta,
                           double *avnorm, int *flag, int *err, int m, int iop, int q, double btol, bool with_avnorm,
@@ -508,12 +540,10 @@ cufsp_status parnoldi_run(PArnoldi **ppa, cufsp_mat *A, const std::vector<double
         const size_t smem = sizeof(double) * ((size_t)chunk + (size_t)std::max(1, m) * grid);
         if (smem > (size_t)device_info().max_smem_optin - sizeof(PSmem) - 1024)
             return set_error(CUFSP_ERR_UNSUPPORTED, "persistent Arnoldi: vector slice exceeds shared memory");
-        // The attribute is process-wide: set it once to the most any driver may ask for, so that
-        // drivers of different sizes on different host threads never undercut each other.
-        static const cudaError_t attr = cudaFuncSetAttribute(
-            (const void *)k_arnoldi_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize,
-            device_info().max_smem_optin - (int)sizeof(PSmem) - 1024);
-        CUFSP_CUDA_TRY(attr);
+        // The attribute belongs to the current device: set it once per device, to the most any
+        // driver may ask for, so that drivers of different sizes on different host threads never
+        // undercut each other.
+        CUFSP_CUDA_TRY(persistent_smem_attribute());
         int per_sm = 0;
         CUFSP_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k_arnoldi_persistent,
                                                                      kPThreads, smem));

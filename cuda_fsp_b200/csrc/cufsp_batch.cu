@@ -226,7 +226,7 @@ cufsp_status ensure_work(cufsp_batch *B, int n_clusters) {
     if (B->d_work) cudaFree(B->d_work);
     B->d_work = nullptr;
     B->work_doubles = 0;
-    CUFSP_CUDA_TRY(cudaMalloc(&B->d_work, sizeof(double) * need));
+    CUFSP_CUDA_TRY(dev_malloc(&B->d_work, sizeof(double) * need));
     B->work_doubles = need;
     return CUFSP_SUCCESS;
 }
@@ -308,7 +308,7 @@ cufsp_status autotune(cufsp_batch *B, double t_final, const double *p, cudaStrea
         const Shape cands[] = {{8, 256, 1}, {16, 256, 1}, {4, 512, 1}, {8, 512, 1},
                                {16, 512, 1}, {8, 256, 2}, {16, 256, 2}};
         const int64_t total = B->offsets.back();
-        if (!B->d_scratch) CUFSP_CUDA_TRY(cudaMalloc(&B->d_scratch, sizeof(double) * (size_t)total));
+        if (!B->d_scratch) CUFSP_CUDA_TRY(dev_malloc(&B->d_scratch, sizeof(double) * (size_t)total));
         double best = 1e300;
         cudaEvent_t e0, e1;
         CUFSP_CUDA_TRY(cudaEventCreate(&e0));
@@ -466,12 +466,12 @@ extern "C" cufsp_status cufsp_batch_create(const cufsp_batch_desc *d, int m, dou
     for (int i = 0; i < ni; ++i)
         std::memcpy(tabs.data() + tab_off_inst[i], d->factor_tables[i],
                     sizeof(double) * (size_t)(tab_off_inst[i + 1] - tab_off_inst[i]));
-    cudaError_t e = cudaMalloc(&B->d_inst, sizeof(CufspBatchInst) * ni);
-    if (e == cudaSuccess) e = cudaMalloc(&B->d_order, sizeof(int) * ni);
-    if (e == cudaSuccess) e = cudaMalloc(&B->d_order_sample, sizeof(int) * B->n_sample);
-    if (e == cudaSuccess) e = cudaMalloc(&B->d_tables, sizeof(double) * std::max<size_t>(1, tabs.size()));
-    if (e == cudaSuccess) e = cudaMalloc(&B->d_stats, sizeof(CufspBatchStat) * ni);
-    if (e == cudaSuccess) e = cudaMalloc(&B->d_counter, sizeof(unsigned));
+    cudaError_t e = dev_malloc(&B->d_inst, sizeof(CufspBatchInst) * ni);
+    if (e == cudaSuccess) e = dev_malloc(&B->d_order, sizeof(int) * ni);
+    if (e == cudaSuccess) e = dev_malloc(&B->d_order_sample, sizeof(int) * B->n_sample);
+    if (e == cudaSuccess) e = dev_malloc(&B->d_tables, sizeof(double) * std::max<size_t>(1, tabs.size()));
+    if (e == cudaSuccess) e = dev_malloc(&B->d_stats, sizeof(CufspBatchStat) * ni);
+    if (e == cudaSuccess) e = dev_malloc(&B->d_counter, sizeof(unsigned));
     if (e == cudaSuccess) e = cudaMemcpy(B->d_inst, B->inst.data(), sizeof(CufspBatchInst) * ni, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(B->d_order, B->order.data(), sizeof(int) * ni, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(B->d_order_sample, sample.data(), sizeof(int) * B->n_sample, cudaMemcpyHostToDevice);

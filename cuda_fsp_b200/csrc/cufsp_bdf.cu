@@ -197,7 +197,7 @@ cufsp_status fetch(cufsp_bdf *B, int first, int count, cudaStream_t st) {
     CUFSP_CUDA_TRY(cudaMemcpyAsync(B->h_scal + first, B->d_scal + first, sizeof(double) * count,
                                    cudaMemcpyDeviceToHost, st));
     CUFSP_CUDA_TRY(cudaStreamSynchronize(st));
-    return CUFSP_SUCCESS;
+    return mat_check_watchdog(B->A, "cufsp_bdf_advance");
 }
 
 cufsp_status change_D(cufsp_bdf *B, int k, double rho, cudaStream_t st) {
@@ -450,8 +450,8 @@ extern "C" cufsp_status cufsp_bdf_create(cufsp_mat *A, const double *coefs, doub
     for (int k = 0; k <= kMaxOrder + 1; ++k) B->econst[k] = 1.0 / (k + 1);
     const size_t nvec = kNHist + (size_t)(maxl + 1) + 4;
     cufsp_status s = CUFSP_SUCCESS;
-    if (cudaMalloc(&B->store, sizeof(double) * B->ld * nvec) != cudaSuccess ||
-        cudaMalloc(&B->d_scal, sizeof(double) * kNScal) != cudaSuccess ||
+    if (dev_malloc(&B->store, sizeof(double) * B->ld * nvec) != cudaSuccess ||
+        dev_malloc(&B->d_scal, sizeof(double) * kNScal) != cudaSuccess ||
         cudaMallocHost(&B->h_scal, sizeof(double) * kNScal) != cudaSuccess) {
         cudaGetLastError();
         s = set_error(CUFSP_ERR_ALLOC, "cufsp_bdf_create: device allocation failed");

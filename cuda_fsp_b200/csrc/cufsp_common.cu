@@ -30,13 +30,16 @@ cufsp_status cuda_error(cudaError_t e, const char *what) {
 
 void clear_error() { g_last_error.clear(); }
 
+// A fixed table indexed by device id: entries never move, so references handed out stay valid
+// while other threads look up other devices.
 const DeviceInfo &device_info() {
+    constexpr int kMaxDevices = 64;
     static std::mutex mu;
-    static std::vector<DeviceInfo> cache;
+    static DeviceInfo cache[kMaxDevices];
     int dev = 0;
     cudaGetDevice(&dev);
+    if (dev < 0 || dev >= kMaxDevices) dev = 0;
     std::lock_guard<std::mutex> lk(mu);
-    if ((int)cache.size() <= dev) cache.resize(dev + 1);
     DeviceInfo &d = cache[dev];
     if (d.sm_count == 0) {
         cudaDeviceGetAttribute(&d.sm_count, cudaDevAttrMultiProcessorCount, dev);
@@ -44,6 +47,35 @@ const DeviceInfo &device_info() {
         if (d.sm_count <= 0) d.sm_count = 148;
     }
     return d;
+}
+
+int *watch_word_alloc(int **d_word) {
+    int *h = nullptr;
+    *d_word = nullptr;
+    if (cudaHostAlloc((void **)&h, sizeof(int), cudaHostAllocMapped | cudaHostAllocPortable) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    *h = 0;
+    if (cudaHostGetDevicePointer((void **)d_word, h, 0) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFreeHost(h);
+        *d_word = nullptr;
+        return nullptr;
+    }
+    return h;
+}
+
+void watch_word_free(int *h_word) {
+    if (h_word) cudaFreeHost(h_word);
+}
+
+int watch_word_take(int *h_word) {
+    if (!h_word) return 0;
+    volatile int *w = h_word;
+    const int v = *w;
+    if (v) *w = 0;
+    return v;
 }
 
 FastDiv make_fastdiv(uint32_t d) {
@@ -68,13 +100,18 @@ int stream_grid(int64_t n, int elems_per_thread, int max_ctas) {
 // Krylov drivers are typically created and destroyed once per solve (the reference's usage); with
 // plain cudaMalloc/cudaFree every solve pays the driver's page-table work and an implicit device
 // synchronisation per buffer (2-6 ms per small solve measured).  Their buffers come from this cache
-// instead: a released buffer is kept (after a device synchronisation, since kernels may still use
-// it) and handed to the next request of a similar size on the same device.
+// instead: a released buffer is kept and handed to the next request of a similar size on the same
+// device.  Work still queued may use a released buffer, so its reuse waits for it: a release that
+// names the stream all uses were ordered on records an event there, and the next owner waits for
+// that event only (other streams keep running); a release without a stream synchronises the
+// buffer's own device.  Idle buffers are kept up to CUFSP_CACHE_MAX_MB (default 1024) per process
+// and returned to the driver by cufsp_cache_trim() or when an allocation of this library fails.
 namespace {
 struct CachedBlock {
     void *p;
     size_t bytes;
     int dev;
+    cudaEvent_t ready;  // recorded at release on the releasing stream; null after a device sync
 };
 struct BufferCache {
     std::mutex mu;
@@ -86,8 +123,68 @@ BufferCache &buffer_cache() {
     static BufferCache *c = new BufferCache();  // never destroyed: no CUDA calls at process exit
     return *c;
 }
-constexpr size_t kCacheCap = (size_t)1 << 30;  // idle bytes kept at most
+size_t cache_cap() {
+    static const size_t cap = [] {
+        const char *e = getenv("CUFSP_CACHE_MAX_MB");
+        const long long mb = e ? atoll(e) : 1024;
+        return (size_t)(mb < 0 ? 0 : mb) << 20;
+    }();
+    return cap;
+}
+
+// Runs f with device `dev` current and restores the caller's device.
+template <class F>
+void on_device(int dev, F f) {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (cur != dev) cudaSetDevice(dev);
+    f();
+    if (cur != dev && cur >= 0) cudaSetDevice(cur);
+}
+
+// Frees the idle blocks of device `dev` (all devices when dev < 0); the caller holds c.mu.
+size_t trim_locked(BufferCache &c, int dev) {
+    size_t freed = 0;
+    for (auto it = c.idle.begin(); it != c.idle.end();) {
+        if (dev < 0 || it->second.dev == dev) {
+            CachedBlock b = it->second;
+            on_device(b.dev, [&] {
+                if (b.ready) {
+                    cudaEventSynchronize(b.ready);
+                    cudaEventDestroy(b.ready);
+                }
+                cudaFree(b.p);
+            });
+            c.idle_bytes -= b.bytes;
+            freed += b.bytes;
+            it = c.idle.erase(it);
+        } else {
+            ++it;
+        }
+    }
+    return freed;
+}
 }  // namespace
+
+cudaError_t dev_malloc(void **p, size_t bytes) {
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaErrorMemoryAllocation) return e;
+    cudaGetLastError();
+    int dev = 0;
+    cudaGetDevice(&dev);
+    BufferCache &c = buffer_cache();
+    {
+        std::lock_guard<std::mutex> lk(c.mu);
+        if (trim_locked(c, dev) == 0) return e;
+    }
+    return cudaMalloc(p, bytes);
+}
+
+size_t cache_trim_all() {
+    BufferCache &c = buffer_cache();
+    std::lock_guard<std::mutex> lk(c.mu);
+    return trim_locked(c, -1);
+}
 
 cudaError_t cache_alloc(void **p, size_t bytes) {
     *p = nullptr;
@@ -97,39 +194,39 @@ cudaError_t cache_alloc(void **p, size_t bytes) {
     if (e != cudaSuccess) return e;
     BufferCache &c = buffer_cache();
     {
-        std::lock_guard<std::mutex> lk(c.mu);
-        for (auto it = c.idle.lower_bound(bytes); it != c.idle.end() && it->first <= 2 * bytes; ++it) {
-            if (it->second.dev != dev) continue;
-            CachedBlock b = it->second;
-            c.idle.erase(it);
-            c.idle_bytes -= b.bytes;
+        CachedBlock b{nullptr, 0, 0, nullptr};
+        {
+            std::lock_guard<std::mutex> lk(c.mu);
+            for (auto it = c.idle.lower_bound(bytes); it != c.idle.end() && it->first <= 2 * bytes; ++it) {
+                if (it->second.dev != dev) continue;
+                b = it->second;
+                c.idle.erase(it);
+                c.idle_bytes -= b.bytes;
+                break;
+            }
+        }
+        if (b.p) {
+            if (b.ready) {  // the previous owner's work on its stream may still use the buffer
+                e = cudaEventSynchronize(b.ready);
+                cudaEventDestroy(b.ready);
+                b.ready = nullptr;
+                if (e != cudaSuccess) return e;
+            }
+            std::lock_guard<std::mutex> lk(c.mu);
             c.live[b.p] = b;
             *p = b.p;
             return cudaSuccess;
         }
     }
-    e = cudaMalloc(p, bytes);
-    if (e == cudaErrorMemoryAllocation) {  // give the idle buffers of this device back and retry
-        cudaGetLastError();
-        std::lock_guard<std::mutex> lk(c.mu);
-        for (auto it = c.idle.begin(); it != c.idle.end();) {
-            if (it->second.dev == dev) {
-                cudaFree(it->second.p);
-                c.idle_bytes -= it->second.bytes;
-                it = c.idle.erase(it);
-            } else {
-                ++it;
-            }
-        }
-        e = cudaMalloc(p, bytes);
-    }
+    e = dev_malloc(p, bytes);
     if (e != cudaSuccess) return e;
     std::lock_guard<std::mutex> lk(c.mu);
-    c.live[*p] = CachedBlock{*p, bytes, dev};
+    c.live[*p] = CachedBlock{*p, bytes, dev, nullptr};
     return cudaSuccess;
 }
 
-void cache_free(void *p) {
+namespace {
+void cache_release(void *p, bool have_stream, cudaStream_t st) {
     if (!p) return;
     BufferCache &c = buffer_cache();
     CachedBlock b;
@@ -143,15 +240,36 @@ void cache_free(void *p) {
         b = it->second;
         c.live.erase(it);
     }
-    cudaDeviceSynchronize();  // work still queued may use the buffer
+    bool keep = true;
+    on_device(b.dev, [&] {
+        b.ready = nullptr;
+        if (have_stream && cudaEventCreateWithFlags(&b.ready, cudaEventDisableTiming) == cudaSuccess) {
+            if (cudaEventRecord(b.ready, st) != cudaSuccess) {
+                cudaGetLastError();
+                cudaEventDestroy(b.ready);
+                b.ready = nullptr;
+            }
+        }
+        if (!b.ready) cudaDeviceSynchronize();  // work still queued on this device may use the buffer
+        std::lock_guard<std::mutex> lk(c.mu);
+        if (c.idle_bytes + b.bytes > cache_cap()) {
+            if (b.ready) {
+                cudaEventSynchronize(b.ready);
+                cudaEventDestroy(b.ready);
+            }
+            cudaFree(b.p);
+            keep = false;
+        }
+    });
+    if (!keep) return;
     std::lock_guard<std::mutex> lk(c.mu);
-    if (c.idle_bytes + b.bytes > kCacheCap) {
-        cudaFree(b.p);
-        return;
-    }
     c.idle.emplace(b.bytes, b);
     c.idle_bytes += b.bytes;
 }
+}  // namespace
+
+void cache_free(void *p) { cache_release(p, false, nullptr); }
+void cache_free(void *p, cudaStream_t last_use) { cache_release(p, true, last_use); }
 
 cufsp_status ReduceScratch::init(int ctas, int k) {
     release();
@@ -166,6 +284,13 @@ cufsp_status ReduceScratch::init(int ctas, int k) {
 void ReduceScratch::release() {
     cache_free(partials);
     cache_free(counter);
+    partials = nullptr;
+    counter = nullptr;
+}
+
+void ReduceScratch::release(cudaStream_t last_use) {
+    cache_free(partials, last_use);
+    cache_free(counter, last_use);
     partials = nullptr;
     counter = nullptr;
 }
@@ -321,6 +446,12 @@ using namespace cufsp;
 
 // ---- C ABI: status and indexing --------------------------------------------------------------
 
+extern "C" cufsp_status cufsp_cache_trim(size_t *freed_bytes) {
+    const size_t f = cufsp::cache_trim_all();
+    if (freed_bytes) *freed_bytes = f;
+    return CUFSP_SUCCESS;
+}
+
 extern "C" const char *cufsp_status_string(cufsp_status s) {
     switch (s) {
         case CUFSP_SUCCESS: return "CUFSP_SUCCESS";
@@ -394,7 +525,7 @@ extern "C" cufsp_status cufsp_vec_sum(int64_t n, const double *x, double *out, c
     cufsp_status s = rs.init(device_info().sm_count * 4, 1);
     if (s != CUFSP_SUCCESS) { rs.release(); return s; }
     double *d_out = nullptr;
-    if (cudaMalloc(&d_out, sizeof(double)) != cudaSuccess) { rs.release(); return set_error(CUFSP_ERR_ALLOC, "cudaMalloc"); }
+    if (dev_malloc(&d_out, sizeof(double)) != cudaSuccess) { rs.release(); return set_error(CUFSP_ERR_ALLOC, "cudaMalloc"); }
     s = launch_sum(n, x, d_out, rs, (cudaStream_t)stream);
     if (s == CUFSP_SUCCESS) {
         cudaError_t e = cudaMemcpyAsync(out, d_out, sizeof(double), cudaMemcpyDeviceToHost, (cudaStream_t)stream);

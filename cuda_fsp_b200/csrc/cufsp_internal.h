@@ -55,13 +55,30 @@ __host__ __device__ __forceinline__ uint32_t fd_div(uint32_t n, const FastDiv &f
 }
 #endif
 
-// Reduction scratch shared by the vector kernels of one handle: per-CTA partials and a
-// completion counter for the last-CTA-reduces pattern (deterministic summation order).
-// Device buffers from a per-process cache (cufsp_common.cu): cache_free synchronises the device and
-// keeps the buffer for the next cache_alloc of a similar size on the same device.
+// Device buffers from a per-process cache (cufsp_common.cu).  cache_free(p, st): every use of p was
+// ordered on stream st; the buffer is kept and its next owner waits for st to reach this point.
+// cache_free(p): uses unknown; synchronises p's device first.  dev_malloc: cudaMalloc that returns
+// the cache's idle buffers of the current device to the driver and retries when memory runs out.
 cudaError_t cache_alloc(void **p, size_t bytes);
 void cache_free(void *p);
+void cache_free(void *p, cudaStream_t last_use);
+cudaError_t dev_malloc(void **p, size_t bytes);
+size_t cache_trim_all();
+template <class T>
+cudaError_t dev_malloc(T **p, size_t bytes) {
+    return dev_malloc(reinterpret_cast<void **>(p), bytes);
+}
 
+// Watchdog word of a kernel with bounded waits: pinned host memory mapped into the device, so the
+// host reads it after any synchronisation of the launching stream without another copy.
+// Returns the host address (0 written) and the device address in *d_word; nullptr on failure.
+int *watch_word_alloc(int **d_word);
+void watch_word_free(int *h_word);
+// Reads and clears a watchdog word (the caller has synchronised the stream of the kernels using it).
+int watch_word_take(int *h_word);
+
+// Reduction scratch shared by the vector kernels of one handle: per-CTA partials and a
+// completion counter for the last-CTA-reduces pattern (deterministic summation order).
 struct ReduceScratch {
     double *partials = nullptr;  // [max_ctas * max_k]
     unsigned int *counter = nullptr;
@@ -69,6 +86,7 @@ struct ReduceScratch {
     int max_k = 0;
     cufsp_status init(int max_ctas, int max_k);
     void release();
+    void release(cudaStream_t last_use);
 };
 
 // Grid for a streaming vector kernel of n elements with 256 threads per CTA.
@@ -107,7 +125,8 @@ void kron_destroy(KronData *k);
 cufsp_status kron_apply(KronData *k, const double *coefs, double alpha, const double *d_alpha,
                         const int *d_skip, const double *x, bool accumulate, double *y, cudaStream_t st,
                         int64_t i_begin = 0, int64_t i_end = -1);
-// Watchdog of the TMA-fed kernel: 1 if a bounded barrier wait expired since the last call (reset).
+// Watchdog of the TMA-fed kernels: 1 if a bounded barrier wait expired since the last call (reset).
+// Does not synchronise: the caller has synchronised the streams the generator's kernels ran on.
 int kron_watchdog(KronData *k);
 // halo (max |shift|) and slab granularity for the host-buffer pipeline
 int64_t kron_halo(const KronData *k);
@@ -129,7 +148,7 @@ PlaneData *plane_create(const ModelHost &m, const double *d_tables, std::string 
 void plane_destroy(PlaneData *pd);
 const std::string &plane_description(const PlaneData *pd);
 int64_t plane_size(const PlaneData *pd);  // states per plane (slab granularity)
-int plane_watchdog(PlaneData *pd);         // 1 if a bounded barrier wait expired since the last call (reset)
+int plane_watchdog(PlaneData *pd);         // 1 if a bounded barrier wait expired since the last call (reset; no sync)
 // false when this apply is not for the plane kernel (range not whole planes, unaligned vectors);
 // otherwise launches and sets *status.
 bool plane_launch(PlaneData *pd, const double *coefs, double alpha, const double *d_alpha, const int *d_skip,
@@ -179,6 +198,9 @@ cufsp_status mat_apply(cufsp_mat *A, const double *coefs, double alpha, const do
                        const double *x, bool accumulate, double *y, cudaStream_t st, int64_t i_begin = 0,
                        int64_t i_end = -1);
 cufsp_status mat_coefs(cufsp_mat *A, double t, const double *coefs_in, std::vector<double> &out);
+// CUFSP_ERR_CUDA when one of the generator's kernels gave up a bounded wait since the last check
+// (its output is then incomplete); called by the drivers after they synchronise their stream.
+cufsp_status mat_check_watchdog(cufsp_mat *A, const char *where);
 // Bring the generator's coefficient-dependent device tables up to `coefs` (stream order); applies
 // captured in a CUDA graph after this call launch nothing else.
 cufsp_status mat_prepare(cufsp_mat *A, const double *coefs, cudaStream_t st);
@@ -197,6 +219,7 @@ cufsp_status parnoldi_run(PArnoldi **pa, cufsp_mat *A, const std::vector<double>
                           double *avnorm, int *flag, int *err, int m, int iop, int q, double btol, bool with_avnorm,
                           cudaStream_t st);
 void parnoldi_destroy(PArnoldi *pa);
+void parnoldi_destroy(PArnoldi *pa, cudaStream_t last_use);  // every launch of pa was ordered on last_use
 // Host threads that run many solves concurrently keep the launch sequence: the persistent pass
 // wants every SM to itself.
 void parnoldi_thread_disable(bool off);

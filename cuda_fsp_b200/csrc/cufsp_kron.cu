@@ -306,7 +306,7 @@ struct KronData {
     MarchArgs ma;       // constant part of the launch arguments
     int march_V = 1, march_threads = 0, march_grid = 0;
     size_t march_smem = 0;
-    int *d_err = nullptr;
+    int *h_err = nullptr, *d_err = nullptr;  // watchdog word of the march kernel (mapped host memory)
     double2 *d_gtab_march = nullptr;  // only when the marching split differs from k
     // runtime-specialised plane kernel (cufsp_kron_plane.cu), when the network has its shape
     PlaneData *plane = nullptr;
@@ -453,8 +453,7 @@ static void plan_march(const ModelHost &m, KronData *kd) {
     const int zsegs = std::max(1, std::min(Z, resident / a.row_tiles));
     a.zseg = (Z + zsegs - 1) / zsegs;
     kd->march_grid = a.row_tiles * ((Z + a.zseg - 1) / a.zseg);
-    if (cudaMalloc(&kd->d_err, sizeof(int)) != cudaSuccess) return;
-    if (cudaMemset(kd->d_err, 0, sizeof(int)) != cudaSuccess) return;
+    if (!(kd->h_err = watch_word_alloc(&kd->d_err))) return;
     kd->march = true;
 }
 
@@ -621,9 +620,9 @@ cufsp_status kron_create(const ModelHost &m, KronData **out) {
     std::copy(m.tables.begin(), m.tables.end(), tabp.begin());
     std::vector<int> nup((size_t)kd->NR * m.ns, 0);
     std::copy(m.nu.begin(), m.nu.end(), nup.begin());
-    e = cudaMalloc(&kd->d_tables, sizeof(double) * tabp.size());
-    if (e == cudaSuccess) e = cudaMalloc(&kd->d_nu, sizeof(int) * nup.size());
-    if (e == cudaSuccess) e = cudaMalloc(&kd->d_gtab, sizeof(double2) * g.size());
+    e = dev_malloc(&kd->d_tables, sizeof(double) * tabp.size());
+    if (e == cudaSuccess) e = dev_malloc(&kd->d_nu, sizeof(int) * nup.size());
+    if (e == cudaSuccess) e = dev_malloc(&kd->d_gtab, sizeof(double2) * g.size());
     if (e == cudaSuccess) e = cudaMemcpy(kd->d_tables, tabp.data(), sizeof(double) * tabp.size(), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(kd->d_nu, nup.data(), sizeof(int) * nup.size(), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(kd->d_gtab, g.data(), sizeof(double2) * g.size(), cudaMemcpyHostToDevice);
@@ -635,7 +634,7 @@ cufsp_status kron_create(const ModelHost &m, KronData **out) {
     plan_march(m, kd);
     if (kd->march && kd->ma.k != kd->k) {  // the marching split needs its own outer table
         const std::vector<double2> gm = outer_table(m, kd, kd->ma.k);
-        e = cudaMalloc(&kd->d_gtab_march, sizeof(double2) * gm.size());
+        e = dev_malloc(&kd->d_gtab_march, sizeof(double2) * gm.size());
         if (e == cudaSuccess)
             e = cudaMemcpy(kd->d_gtab_march, gm.data(), sizeof(double2) * gm.size(), cudaMemcpyHostToDevice);
         if (e != cudaSuccess) kd->march = false;
@@ -651,20 +650,15 @@ void kron_destroy(KronData *k) {
     if (k->d_nu) cudaFree(k->d_nu);
     if (k->d_gtab) cudaFree(k->d_gtab);
     if (k->d_gtab_march) cudaFree(k->d_gtab_march);
-    if (k->d_err) cudaFree(k->d_err);
+    watch_word_free(k->h_err);
     plane_destroy(k->plane);
     delete k;
 }
 
 int kron_watchdog(KronData *k) {
     if (!k) return 0;
-    int pv = k->plane ? plane_watchdog(k->plane) : 0;
-    if (pv < 0) return -1;
-    if (!k->d_err) return pv;
-    int v = 0;
-    if (cudaMemcpy(&v, k->d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
-    if (v) cudaMemset(k->d_err, 0, sizeof(int));
-    return v | pv;
+    const int pv = k->plane ? plane_watchdog(k->plane) : 0;
+    return watch_word_take(k->h_err) | pv;
 }
 
 // The plane kernel reads one plane beyond each end of the range it computes.

@@ -134,7 +134,7 @@ struct PlaneData {
     int tab_stride = 0;
     double2 *d_gtab = nullptr;       // outer factors for the species-0 / rest split
     const double *d_tab0 = nullptr;  // species-0 tables inside the generator's table array
-    int *d_err = nullptr;            // watchdog flag of the bounded barrier waits
+    int *h_err = nullptr, *d_err = nullptr;  // watchdog word of the bounded barrier waits (mapped host memory)
     double *d_words = nullptr;       // row words for the coefficients in words_coefs
     std::vector<double> words_coefs;
     WordArgs wa;
@@ -307,7 +307,10 @@ PlaneData *plane_create(const ModelHost &m, const double *d_tables, std::string 
       << fa_tabs.size() << "\n#define CUFSP_PLANE_NFB " << fb_tabs.size() << "\n#define CUFSP_PLANE_NT " << terms.size()
       << "\n#define CUFSP_PLANE_NDG " << dgs.size() << "\n#define CUFSP_PLANE_TR " << tr << "\n#define CUFSP_PLANE_STAGES "
       << stages << "\n#define CUFSP_PLANE_PPS " << pps << "\n#define CUFSP_PLANE_YTMA " << ytma << "\n#define CUFSP_PLANE_ROWS " << (rows ? 1 : 0) << "\n#define CUFSP_PLANE_THREADS " << pd->threads
-      << "\n#define CUFSP_PLANE_MINB " << minb << "\nnamespace cufsp_plane {\n";
+      << "\n#define CUFSP_PLANE_MINB " << minb << "\n";
+    // Tries of the bounded waits before a plane is computed (tests of the watchdog only).
+    if (const char *wt = getenv("CUFSP_PLANE_WAIT_TRIES")) s << "#define CUFSP_PLANE_WAIT_TRIES " << std::max(0, atoi(wt)) << "\n";
+    s << "namespace cufsp_plane {\n";
     emit_fn(s, "nu0", nu0);
     emit_fn(s, "o0", o0);
     emit_fn(s, "o1", o1);
@@ -360,11 +363,10 @@ PlaneData *plane_create(const ModelHost &m, const double *d_tables, std::string 
             g[(size_t)q * nr + r] = make_double2(ok ? ga : 0.0, gb);
         }
     }
-    e = cudaMalloc(&pd->d_gtab, sizeof(double2) * g.size());
+    e = dev_malloc(&pd->d_gtab, sizeof(double2) * g.size());
     if (e == cudaSuccess) e = cudaMemcpy(pd->d_gtab, g.data(), sizeof(double2) * g.size(), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMalloc(&pd->d_err, sizeof(int));
-    if (e == cudaSuccess) e = cudaMalloc(&pd->d_words, sizeof(double) * (size_t)Q * pd->wa.nwp);
-    if (e == cudaSuccess) e = cudaMemset(pd->d_err, 0, sizeof(int));
+    if (e == cudaSuccess && !(pd->h_err = watch_word_alloc(&pd->d_err))) e = cudaErrorMemoryAllocation;
+    if (e == cudaSuccess) e = dev_malloc(&pd->d_words, sizeof(double) * (size_t)Q * pd->wa.nwp);
     if (e != cudaSuccess) {
         cudaGetLastError();
         why = std::string("plane kernel tables: ") + cudaGetErrorString(e);
@@ -383,7 +385,7 @@ PlaneData *plane_create(const ModelHost &m, const double *d_tables, std::string 
 void plane_destroy(PlaneData *pd) {
     if (!pd) return;
     if (pd->d_gtab) cudaFree(pd->d_gtab);
-    if (pd->d_err) cudaFree(pd->d_err);
+    watch_word_free(pd->h_err);
     if (pd->d_words) cudaFree(pd->d_words);
     delete pd;  // the compiled kernels stay in the process cache
 }
@@ -391,12 +393,7 @@ void plane_destroy(PlaneData *pd) {
 const std::string &plane_description(const PlaneData *pd) { return pd->description; }
 int64_t plane_size(const PlaneData *pd) { return (int64_t)pd->n0 * pd->n1; }
 
-int plane_watchdog(PlaneData *pd) {
-    int v = 0;
-    if (cudaMemcpy(&v, pd->d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
-    if (v) cudaMemset(pd->d_err, 0, sizeof(int));
-    return v;
-}
+int plane_watchdog(PlaneData *pd) { return watch_word_take(pd->h_err); }
 
 // Row words for these coefficients, rebuilt in stream order when they change.
 cufsp_status plane_prepare(PlaneData *pd, const double *coefs, cudaStream_t st) {

@@ -210,6 +210,9 @@ struct cufsp_expv_s {
     std::vector<Graph> graphs;
     cudaStream_t cap_stream = nullptr;
     cufsp::PArnoldi *pa = nullptr;  // persistent single-launch Arnoldi pass (small generators)
+    // the stream of the handle's device work; released buffers wait for it alone unless several were used
+    cudaStream_t last_stream = nullptr;
+    bool used = false, mixed = false;
 };
 
 namespace {
@@ -301,6 +304,9 @@ bool graphs_enabled() {
 // step); the generator's coefficient-dependent tables are prepared eagerly before each replay.
 cufsp_status arnoldi_pass(cufsp_expv *E, double *v, cudaStream_t st, bool with_avnorm) {
     cufsp_status s;
+    if (E->used && E->last_stream != st) E->mixed = true;
+    E->used = true;
+    E->last_stream = st;
     const bool persistent = E->A && parnoldi_wanted(E->A, E->n, E->m);
     if (persistent) {
         s = parnoldi_run(&E->pa, E->A, E->coefs, E->transpose, E->n, v, E->W, E->ks.H, E->ks.rho, E->ks.gam,
@@ -350,6 +356,10 @@ cufsp_status arnoldi_pass(cufsp_expv *E, double *v, cudaStream_t st, bool with_a
     std::memcpy(&barrier_err, reinterpret_cast<const char *>(hrho + 2 * mp2 + 4) + sizeof(int), sizeof(int));
     if (persistent && barrier_err)
         return set_error(CUFSP_ERR_CUDA, "expv: a grid barrier wait of the persistent Arnoldi pass expired");
+    if (!persistent && E->A) {
+        s = mat_check_watchdog(E->A, "expv");
+        if (s != CUFSP_SUCCESS) return s;
+    }
     KrylovStep &L = E->last;
     L.mb = flag > 0 ? flag : m;
     L.beta = hrho[2 * mp2];
@@ -538,11 +548,18 @@ extern "C" cufsp_status cufsp_expv_create(int64_t n, int m, double tol, int iop,
 extern "C" cufsp_status cufsp_expv_destroy(cufsp_expv *E) {
     if (!E) return CUFSP_SUCCESS;
     for (auto &g : E->graphs) cudaGraphExecDestroy(g.exec);
-    parnoldi_destroy(E->pa);
+    if (E->used && !E->mixed) {  // every launch of the handle was ordered on one stream
+        parnoldi_destroy(E->pa, E->last_stream);
+        cache_free(E->W, E->last_stream);
+        cache_free(E->d_state, E->last_stream);
+        E->rs.release(E->last_stream);
+    } else {
+        parnoldi_destroy(E->pa);
+        cache_free(E->W);
+        cache_free(E->d_state);
+        E->rs.release();
+    }
     if (E->cap_stream) cudaStreamDestroy(E->cap_stream);
-    cache_free(E->W);
-    cache_free(E->d_state);
-    E->rs.release();
     delete E;
     return CUFSP_SUCCESS;
 }

@@ -112,11 +112,20 @@ extern "C" cufsp_status cufsp_mat_action(cufsp_mat *A, double t, const double *x
 
 extern "C" cufsp_status cufsp_mat_watchdog(cufsp_mat *A, int *tripped) {
     if (!A || !tripped) return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_mat_watchdog: NULL argument");
-    const int v = A->kron ? kron_watchdog(A->kron) : 0;
-    if (v < 0) return set_error(CUFSP_ERR_CUDA, "cufsp_mat_watchdog: device read failed");
-    *tripped = v;
+    CUFSP_CUDA_TRY(cudaDeviceSynchronize());  // every launch of the generator has finished
+    *tripped = A->kron ? kron_watchdog(A->kron) : 0;
     return CUFSP_SUCCESS;
 }
+
+namespace cufsp {
+cufsp_status mat_check_watchdog(cufsp_mat *A, const char *where) {
+    if (A && A->kron && kron_watchdog(A->kron))
+        return set_error(CUFSP_ERR_CUDA, std::string(where) +
+                                             ": a bounded shared-memory barrier wait of the generator kernel expired "
+                                             "(the generator action is incomplete)");
+    return CUFSP_SUCCESS;
+}
+}  // namespace cufsp
 
 extern "C" cufsp_status cufsp_mat_describe(const cufsp_mat *A, char *buf, size_t len) {
     if (!A || !buf || len == 0) return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_mat_describe: bad argument");
@@ -142,8 +151,8 @@ extern "C" cufsp_status cufsp_mat_action_host(cufsp_mat *A, double t, const doub
     const int64_t n = A->model.n;
     const int kSlabs = 8;
     if (!A->d_x) {
-        CUFSP_CUDA_TRY(cudaMalloc(&A->d_x, sizeof(double) * n));
-        CUFSP_CUDA_TRY(cudaMalloc(&A->d_y, sizeof(double) * n));
+        CUFSP_CUDA_TRY(dev_malloc(&A->d_x, sizeof(double) * n));
+        CUFSP_CUDA_TRY(dev_malloc(&A->d_y, sizeof(double) * n));
         CUFSP_CUDA_TRY(cudaStreamCreateWithFlags(&A->s_in, cudaStreamNonBlocking));
         CUFSP_CUDA_TRY(cudaStreamCreateWithFlags(&A->s_comp, cudaStreamNonBlocking));
         CUFSP_CUDA_TRY(cudaStreamCreateWithFlags(&A->s_out, cudaStreamNonBlocking));
@@ -184,5 +193,5 @@ extern "C" cufsp_status cufsp_mat_action_host(cufsp_mat *A, double t, const doub
     }
     CUFSP_CUDA_TRY(cudaStreamSynchronize(A->s_out));
     CUFSP_CUDA_TRY(cudaStreamSynchronize(A->s_comp));
-    return CUFSP_SUCCESS;
+    return mat_check_watchdog(A, "cufsp_mat_action_host");
 }

@@ -105,9 +105,15 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned 
         : "memory");
     return ok != 0;
 }
-// Each try_wait suspends for a hardware-defined interval; false after 2^20 tries.
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long *bar, unsigned parity) {
-    for (int it = 0; it < (1 << 20); ++it)
+// Each try_wait suspends for a hardware-defined interval; false after `tries` tries.  The waits
+// before a plane is computed use CUFSP_PLANE_WAIT_TRIES (2^20 unless the host asks for fewer, which
+// only the watchdog's own test does: 0 makes every such wait give up at once); the final drain of
+// copies still in flight always uses 2^20, so no CTA leaves with a copy outstanding.
+#ifndef CUFSP_PLANE_WAIT_TRIES
+#define CUFSP_PLANE_WAIT_TRIES (1 << 20)
+#endif
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long *bar, unsigned parity, int tries) {
+    for (int it = 0; it < tries; ++it)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }
@@ -340,7 +346,12 @@ __device__ __forceinline__ void plane_mv(const CufspPlaneArgs &a, const double *
     const double alpha = a.alpha * (a.d_alpha ? __ldg(a.d_alpha) : 1.0);
 
     auto stage_of = [&](int p) { return smem + ((p - pbase) % S) * sd; };
-    auto wait_plane = [&](int p) -> bool { return mbar_wait_bounded(bars + (p - pbase) % S, ((p - pbase) / S) & 1); };
+    auto wait_plane = [&](int p) -> bool {
+        return mbar_wait_bounded(bars + (p - pbase) % S, ((p - pbase) / S) & 1, CUFSP_PLANE_WAIT_TRIES);
+    };
+    auto drain_plane = [&](int p) -> bool {
+        return mbar_wait_bounded(bars + (p - pbase) % S, ((p - pbase) / S) & 1, 1 << 20);
+    };
 
     bool bad = false;
     Slot q0, q1, q2, q3;
@@ -353,6 +364,7 @@ __device__ __forceinline__ void plane_mv(const CufspPlaneArgs &a, const double *
     }
     __syncthreads();
     bad = failed_flag != 0;
+    const bool prologue_ok = !bad;
 
     int z = t.z0;
     // Refill after a CTA barrier: the stages released by the step go to the next planes.
@@ -420,9 +432,10 @@ __device__ __forceinline__ void plane_mv(const CufspPlaneArgs &a, const double *
         }
     }
     if (tid == 0) {
-        // every issued copy must have landed before the CTA's shared memory is released
-        for (int p = z + 1; p <= issued; ++p)
-            if (!wait_plane(p)) bad = true;
+        // every issued copy must have landed before the CTA's shared memory is released: after a
+        // failed prologue none was waited for; otherwise the planes up to z were
+        for (int p = prologue_ok ? z + 1 : pbase; p <= issued; ++p)
+            if (!drain_plane(p)) bad = true;
         if (bad) atomicExch(a.err, 1);
     }
 }

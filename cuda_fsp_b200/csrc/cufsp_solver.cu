@@ -116,7 +116,7 @@ cufsp_status solver_new(cufsp_mat *A, const double *times, int n_times, double f
 
 cufsp_status solver_finish(cufsp_solver *S, cufsp_status s, cufsp_solver **out) {
     if (s == CUFSP_SUCCESS) s = S->rs.init(device_info().sm_count * 4, 1);
-    if (s == CUFSP_SUCCESS && cudaMalloc(&S->d_sum, sizeof(double)) != cudaSuccess)
+    if (s == CUFSP_SUCCESS && dev_malloc(&S->d_sum, sizeof(double)) != cudaSuccess)
         s = set_error(CUFSP_ERR_ALLOC, "cufsp_solver_create: cudaMalloc");
     if (s != CUFSP_SUCCESS) {
         cufsp_solver_destroy(S);

@@ -163,12 +163,12 @@ cufsp_status sparse_create(const ModelHost &m, SparseData **out) {
     }
     const DeviceInfo &di = device_info();
     sd->grid_full = di.sm_count * 8;
-    cudaError_t e = cudaMalloc(&sd->d_P, sizeof(double) * (size_t)m.nr * (size_t)m.n);
-    if (e == cudaSuccess) e = cudaMalloc(&sd->d_rinfo, sizeof(int) * rinfo.size());
+    cudaError_t e = dev_malloc(&sd->d_P, sizeof(double) * (size_t)m.nr * (size_t)m.n);
+    if (e == cudaSuccess) e = dev_malloc(&sd->d_rinfo, sizeof(int) * rinfo.size());
     if (e == cudaSuccess) e = cudaMemcpy(sd->d_rinfo, rinfo.data(), sizeof(int) * rinfo.size(), cudaMemcpyHostToDevice);
     double *d_tables = nullptr;
     if (e == cudaSuccess && !m.prop_device) {
-        e = cudaMalloc(&d_tables, sizeof(double) * m.tables.size());
+        e = dev_malloc(&d_tables, sizeof(double) * m.tables.size());
         if (e == cudaSuccess)
             e = cudaMemcpy(d_tables, m.tables.data(), sizeof(double) * m.tables.size(), cudaMemcpyHostToDevice);
     }

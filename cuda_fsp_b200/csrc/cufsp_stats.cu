@@ -110,7 +110,7 @@ extern "C" cufsp_status cufsp_loglik(int64_t n, const double *d_p, int64_t block
     const int ctas = device_info().sm_count * 4;
     cufsp_status s = rs.init(ctas, 1);
     double *d_out = nullptr;
-    if (s == CUFSP_SUCCESS && cudaMalloc(&d_out, sizeof(double)) != cudaSuccess)
+    if (s == CUFSP_SUCCESS && dev_malloc(&d_out, sizeof(double)) != cudaSuccess)
         s = set_error(CUFSP_ERR_ALLOC, "cufsp_loglik: cudaMalloc");
     if (s == CUFSP_SUCCESS) {
         const int64_t nk = n / block;
@@ -158,11 +158,11 @@ extern "C" cufsp_status cufsp_ssa(const cufsp_model_desc *desc, const double *co
     double *d_tab = nullptr, *d_times = nullptr;
     int *d_nu = nullptr, *d_x0 = nullptr, *d_err = nullptr;
     cudaStream_t st = (cudaStream_t)stream;
-    cudaError_t e = cudaMalloc(&d_tab, sizeof(double) * m.tables.size());
-    if (e == cudaSuccess) e = cudaMalloc(&d_nu, sizeof(int) * m.nu.size());
-    if (e == cudaSuccess) e = cudaMalloc(&d_x0, sizeof(int) * m.ns);
-    if (e == cudaSuccess) e = cudaMalloc(&d_times, sizeof(double) * n_times);
-    if (e == cudaSuccess) e = cudaMalloc(&d_err, sizeof(int));
+    cudaError_t e = dev_malloc(&d_tab, sizeof(double) * m.tables.size());
+    if (e == cudaSuccess) e = dev_malloc(&d_nu, sizeof(int) * m.nu.size());
+    if (e == cudaSuccess) e = dev_malloc(&d_x0, sizeof(int) * m.ns);
+    if (e == cudaSuccess) e = dev_malloc(&d_times, sizeof(double) * n_times);
+    if (e == cudaSuccess) e = dev_malloc(&d_err, sizeof(int));
     if (e == cudaSuccess) e = cudaMemcpy(d_tab, m.tables.data(), sizeof(double) * m.tables.size(), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(d_nu, m.nu.data(), sizeof(int) * m.nu.size(), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(d_x0, x0, sizeof(int) * m.ns, cudaMemcpyHostToDevice);

@@ -118,7 +118,10 @@ cufsp_status cufsp_mat_action_host(cufsp_mat *A, double t, const double *x_host,
 
 /* Watchdog of the TMA-fed KRONECKER kernel: *tripped = 1 when one of its bounded shared-memory
  * barrier waits expired since the previous call (the affected output is then incomplete); the flag
- * is reset.  Synchronises the device. */
+ * is reset.  Synchronises the device.  The drivers that synchronise anyway -- Krylov steps, BDF steps,
+ * the FSP solvers, the gradient and cufsp_mat_action_host -- read the same flag after every step and
+ * return CUFSP_ERR_CUDA when it is set; a caller of the asynchronous cufsp_mat_action/apply checks it
+ * here. */
 cufsp_status cufsp_mat_watchdog(cufsp_mat *A, int *tripped);
 
 /* Which kernel serves this generator's action, as text (e.g. the runtime-specialised plane kernel of
@@ -362,6 +365,13 @@ cufsp_status cufsp_expm_host(int k, const double *A, double *F);
 /* ---- vector helpers (device) ------------------------------------------------------------- */
 /* sum of x (deterministic order); result written to host *out; synchronises `stream`. */
 cufsp_status cufsp_vec_sum(int64_t n, const double *x, double *out, cufsp_stream_t stream);
+
+/* Device buffers of released Krylov, adjoint and persistent-pass workspaces are kept in a per-process
+ * cache for reuse (up to CUFSP_CACHE_MAX_MB megabytes, default 1024, read once from the environment);
+ * an allocation of this library that runs out of memory returns that device's idle buffers and
+ * retries.  This returns every idle buffer of every device to the driver now (e.g. before a caller's
+ * own large allocation); *freed_bytes (nullable) receives the amount.  No counterpart in the reference. */
+cufsp_status cufsp_cache_trim(size_t *freed_bytes);
 
 /* d_dst[0..n) = d_src[0..n) (device to device), ordered on `stream`. */
 cufsp_status cufsp_vec_copy(int64_t n, const double *d_src, double *d_dst, cufsp_stream_t stream);

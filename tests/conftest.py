@@ -42,3 +42,16 @@ def testmodels(built):
     lib.tm_toggle_propfn.restype = C.c_void_p
     lib.tm_nonfact_propfn.restype = C.c_void_p
     return lib
+
+
+def require_ref():
+    """The reference's own compiled code (oracle/_ref/libref.so, built by oracle/Makefile from the
+    reference sources and shipped with the tree).  Its absence fails the test: the comparisons with
+    the reference's kernels and host functions are the strongest parity evidence and must not
+    vanish from a green run."""
+    import oracle
+    R = oracle.ref()
+    if R is None:
+        pytest.fail(f"{oracle.REF_SO} is missing: build it with `make -C oracle ref` where the reference "
+                    "sources are present (CUFSP_REFERENCE_SRC) and ship it with the tree")
+    return R

@@ -1,0 +1,122 @@
+"""Parity at the benchmark workloads' own sizes (gpu), against the FP64 oracle.
+
+The other GPU tests check every path on small boxes; these take the same paths at the sizes the
+benchmark legs run, where step counts, grids, launch shapes and rounding differ:
+  * batched Krylov over gene_batch(256) instances whose mRNA bounds span 63..255 (t = 30), and the
+    single-instance path on the same instances, each against a tol = 1e-13 oracle solution;
+  * the adjoint gradient on the 131,072-state gene box against forward sensitivities integrated by
+    the oracle's Krylov expv;
+  * the BDF path on the 131,072-state time-varying gene model against the oracle's BDF;
+  * Krylov steps through the overwrite-form plane kernel on a 128^3 box of the 255^3 workload's
+    network (above the persistent pass's 2^20 states) against the oracle.
+Reference anchor for the Krylov value checks: tests/test_kry_expv.cu:98-110 of the reference (its
+only value-level Krylov check is mass conservation; values are pinned here through the oracle's
+restatement of KryExpvFSP).
+"""
+import numpy as np
+import pytest
+
+import oracle
+from cuda_fsp_b200 import (BatchKrylov, BDFIntegrator, FSPMat, KryExpvFSP, Likelihood, MatrixFormat,
+                           generate_data, histograms, models)
+
+pytestmark = pytest.mark.gpu
+
+KRYLOV_BAR = 1e-8  # expmv within the Krylov tolerance in 1-norm
+GRAD_RTOL = 1e-6
+
+
+def dev(a):
+    import torch
+    return torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device="cuda")
+
+
+def c4_instances():
+    """Four instances of the batched workload (gene_batch(256): rates within a decade of nominal,
+    mRNA bounds 63..255): the smallest and the largest box, and instances 0 and 128, two of the four
+    the batched leg compares with the single-instance path."""
+    ms = models.gene_batch(256)
+    order = sorted(range(len(ms)), key=lambda i: ms[i].n_states)
+    pick = [order[0], 0, 128, order[-1]]
+    return [ms[i] for i in pick]
+
+
+def test_c4_batched_and_single_at_full_bounds(cuda):
+    ms = c4_instances()
+    bounds = [b for mm in ms for b in mm.bounds[3:]]
+    assert min(bounds) <= 70 and max(bounds) >= 250  # the instances span the 63..255 range
+    B = BatchKrylov.from_models(ms, m=30, tol=1e-8)
+    B.set_shape(4, 512)
+    p = B.pack([mm.p0() for mm in ms])
+    stats = B.solve(30.0, p)
+    out = B.unpack(p)
+    errs = []
+    for mm, w, st in zip(ms, out, stats):
+        truth, _, rc = oracle.expv(oracle.assemble_model(mm), mm.coefs(0), 30.0, mm.p0(), m=40, tol=1e-13,
+                                   max_nstep=10**6)
+        assert rc == 0
+        A = FSPMat.from_model(mm, MatrixFormat.KRONECKER)
+        v = dev(mm.p0())
+        KryExpvFSP(30.0, A, v, m=30, tol=1e-8, coefs=mm.coefs(0)).solve()
+        e_batch = float(np.abs(w - truth).sum())
+        e_single = float(np.abs(v.cpu().numpy() - truth).sum())
+        errs.append((mm.bounds[3:], e_batch, e_single))
+        assert st["status"] == 0 and st["t"] == 30.0
+    for b, e_batch, e_single in errs:
+        assert e_batch <= KRYLOV_BAR, errs
+        assert e_single <= KRYLOV_BAR, errs
+
+
+def test_c5_gradient_on_full_gene_box(cuda):
+    """d log L / d log theta on the 131,072-state box (1,000 seeded-SSA cells at 8 log-spaced times
+    in [1, 60], marginalised over the gene states) against forward sensitivities for three rates: a
+    gene switch, a transcription and a degradation."""
+    m = models.gene_expression((1, 1, 1, 127, 127), time_varying=False)
+    times = np.geomspace(1.0, 60.0, 8)
+    snaps = generate_data(m, times, [0, 0, 0, 0, 0], 1000, seed=20261205)
+    counts, outside = histograms(snaps, m.bounds, n_marginal=3)
+    L = Likelihood(m, times, counts, outside=outside, n_marginal=3, kry_tol=1e-10)
+    ll, g = L.gradient()
+    rates = [0, 8, 11]
+    ll_ref, g_ref = oracle.loglik_grad_forward_krylov(oracle.assemble_model(m), m.coefs(0), times, m.p0(), counts,
+                                                      8, rates, m=40, tol=1e-12)
+    ll_ref += outside.sum() * np.log(1e-44)
+    assert abs(ll - ll_ref) <= 1e-8 * abs(ll_ref)
+    for r in rates:
+        assert abs(g[r] - g_ref[r]) <= GRAD_RTOL * abs(g_ref[r]), (r, g[r], g_ref[r])
+
+
+def test_c2_bdf_on_full_gene_box(cuda):
+    """The time-varying gene model on its full 131,072-state box over [0, 6] (the switch at t = 5),
+    rtol 1e-8, atol 1e-14: the device BDF against the oracle's BDF (the bar of the small-box BDF tests)."""
+    m = models.gene_expression((1, 1, 1, 127, 127), time_varying=True)
+    times = [2.0, 6.0]
+    A = FSPMat.from_model(m, MatrixFormat.KRONECKER)
+    Bi = BDFIntegrator(A, rtol=1e-8, atol=1e-14)
+    p = dev(m.p0())
+    Bi.init(0.0, p)
+    got = []
+    for t in times:
+        assert Bi.advance(t, p) == t
+        got.append(p.cpu().numpy().copy())
+    ref, rst, rc = oracle.bdf(oracle.assemble_model(m), m.coefs, 0.0, m.p0(), times, rtol=1e-8, atol=1e-14)
+    assert rc == 0
+    for k in range(len(times)):
+        assert np.abs(got[k] - ref[k]).sum() <= 1e-7, (k, np.abs(got[k] - ref[k]).sum())
+        assert abs(got[k].sum() - ref[k].sum()) <= 1e-10
+    assert abs(Bi.stats["n_steps"] - rst["n_steps"]) <= max(3, rst["n_steps"] // 20)
+
+
+def test_c3_krylov_steps_through_plane_kernel(cuda):
+    """The 255^3 workload's network and initial distribution on a 128^3 box (2,097,152 states, above
+    the persistent pass's limit, so every Arnoldi matvec is the overwrite-form plane kernel in a
+    replayed graph): exp(tA) p0 to t = 0.006 (several Krylov steps) against the oracle."""
+    m = models.mass_action_3(bounds=(127, 127, 127))
+    A = FSPMat.from_model(m, MatrixFormat.KRONECKER)
+    assert "plane kernel" in A.describe()
+    v = dev(m.p0())
+    st = KryExpvFSP(0.006, A, v, m=30, tol=1e-8, coefs=m.coefs(0)).solve()
+    w, st_ref, rc = oracle.expv(oracle.assemble_model(m), m.coefs(0), 0.006, m.p0(), m=30, tol=1e-8)
+    assert rc == 0 and st["t_now"] == 0.006 and st["n_steps"] >= 3
+    assert np.abs(v.cpu().numpy() - w).sum() <= KRYLOV_BAR
+    assert abs(st["n_steps"] - st_ref["n_steps"]) <= 1

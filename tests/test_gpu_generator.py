@@ -5,6 +5,7 @@ import numpy as np
 import pytest
 
 import oracle
+from conftest import require_ref
 from cuda_fsp_b200 import FSPMat, MatrixFormat, get_states, models
 
 pytestmark = pytest.mark.gpu
@@ -192,9 +193,7 @@ def test_kron_equals_hyb_reference_tolerances(cuda):
 def test_against_reference_gpu_kernels(cuda):
     """The reference's own HYB and Kronecker kernels (built from its sources into oracle/_ref) on
     sizes they handle (multiples of 1024 states)."""
-    R = oracle.ref()
-    if R is None:
-        pytest.skip("reference shim not built")
+    R = require_ref()
     rng = np.random.default_rng(11)
     # HYB with the toggle PropFun, 32x32 = 1024 states
     m = models.toggle((31, 31))
@@ -251,17 +250,16 @@ def test_full_size_properties(cuda):
     yp = torch.zeros_like(p)
     A.apply(p, yp, coefs=c)
     assert yp.sum().item() <= 1e-12
-    R = oracle.ref()
-    if R is not None:
-        b = np.asarray(m.bounds, np.int32)
-        sv, sc, sr = m.stoich_csr()
-        tab = np.ascontiguousarray(m.tables)
-        cc = np.ascontiguousarray(c)
-        xh = x1.cpu().numpy()
-        y_ref = np.zeros(n)
-        assert R.ref_gpu_kron(m.ns, m.nr, b.ctypes.data, sv.ctypes.data, sc.ctypes.data, sr.ctypes.data, tab.ctypes.data,
-                              cc.ctypes.data, xh.ctypes.data, y_ref.ctypes.data) == 0
-        assert np.abs(host(y1) - y_ref).max() <= MATVEC_RTOL * 2 * bound
+    R = require_ref()
+    b = np.asarray(m.bounds, np.int32)
+    sv, sc, sr = m.stoich_csr()
+    tab = np.ascontiguousarray(m.tables)
+    cc = np.ascontiguousarray(c)
+    xh = x1.cpu().numpy()
+    y_ref = np.zeros(n)
+    assert R.ref_gpu_kron(m.ns, m.nr, b.ctypes.data, sv.ctypes.data, sc.ctypes.data, sr.ctypes.data, tab.ctypes.data,
+                          cc.ctypes.data, xh.ctypes.data, y_ref.ctypes.data) == 0
+    assert np.abs(host(y1) - y_ref).max() <= MATVEC_RTOL * 2 * bound
 
 
 def test_action_host_buffers(cuda):
@@ -287,9 +285,8 @@ def test_enumeration_known_answer_on_gpu(cuda):
     for b in ([1023, 1023, 3], [6, 0, 9, 2], [100000], [1, 1, 1, 127, 127]):
         got = get_states(b).cpu().numpy()
         assert np.array_equal(got, oracle.get_states(b))
-    R = oracle.ref()
-    if R is not None:
-        b = np.asarray([1023, 1023, 3], np.int32)
-        out = np.empty((1024 * 1024 * 4, 3), np.int32)
-        assert R.ref_gpu_get_states(3, b.ctypes.data, out.ctypes.data) == 0
-        assert np.array_equal(out, oracle.get_states(b))
+    R = require_ref()
+    b = np.asarray([1023, 1023, 3], np.int32)
+    out = np.empty((1024 * 1024 * 4, 3), np.int32)
+    assert R.ref_gpu_get_states(3, b.ctypes.data, out.ctypes.data) == 0
+    assert np.array_equal(out, oracle.get_states(b))

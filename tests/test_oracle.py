@@ -3,6 +3,7 @@ import numpy as np
 import pytest
 
 import oracle
+from conftest import require_ref
 from cuda_fsp_b200 import models
 
 
@@ -20,9 +21,7 @@ def test_enumeration_known_answer():
 def test_indexing_matches_reference_host_code(bounds):
     """indx2state / state2indx / rect_fsp_num_states (src/cme_util.cu:5-22,55-62) run from the
     reference's own compiled objects, against the restatement."""
-    R = oracle.ref()
-    if R is None:
-        pytest.skip("reference shim not built (reference sources absent)")
+    R = require_ref()
     b = np.asarray(bounds, np.int32)
     n = oracle.num_states(b)
     assert R.ref_num_states(len(b), b.ctypes.data) == n
@@ -40,9 +39,7 @@ def test_indexing_matches_reference_host_code(bounds):
 def test_factor_table_layout_matches_reference():
     """fspmat_sdkron_fill_host_data (src/fspmat_kron_kernels.cu:170-190) fills the same table
     layout the product consumes, and its offsets are -nu."""
-    R = oracle.ref()
-    if R is None:
-        pytest.skip("reference shim not built (reference sources absent)")
+    R = require_ref()
     for m in (models.toggle((31, 31)), models.gene_expression((1, 1, 1, 7, 9)), models.mass_action_3(6)):
         b = np.asarray(m.bounds, np.int32)
         sv, sc, sr = m.stoich_csr()
