@@ -79,11 +79,16 @@ class ClockSampler:
 
     def __init__(self, index: int):
         self.index = index
-        self.samples: list[float] = []
+        self.samples: list[tuple[float, float]] = []  # (time, MHz)
         self.reasons: set[str] = set()
+        self.marks: list[float] = []
         self.smax = None
         self._stop = threading.Event()
         self.nvml = None
+
+    def mark(self):
+        """Start / end of the timed window inside the sampled period."""
+        self.marks.append(time.perf_counter())
 
     def start(self):
         try:
@@ -102,22 +107,33 @@ class ClockSampler:
         pv = self.nvml
         while not self._stop.is_set():
             try:
-                self.samples.append(float(pv.nvmlDeviceGetClockInfo(self.h, pv.NVML_CLOCK_SM)))
+                self.samples.append((time.perf_counter(), float(pv.nvmlDeviceGetClockInfo(self.h, pv.NVML_CLOCK_SM))))
                 r = pv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
                 for bit, name in self.REASONS.items():
                     if r & bit:
                         self.reasons.add(name)
             except Exception:
                 pass
-            time.sleep(0.001)
+            time.sleep(0.0002)
 
     def stop(self) -> dict:
         if self.nvml is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvml unavailable"], "samples": 0}
         self._stop.set()
         self.t.join(timeout=2)
-        return {"sm_mhz": statistics.median(self.samples) if self.samples else None, "sm_max_mhz": self.smax,
-                "reasons": sorted(self.reasons), "samples": len(self.samples)}
+        mhz = [v for _, v in self.samples]
+        out = {"sm_mhz": statistics.median(mhz) if mhz else None, "sm_max_mhz": self.smax,
+               "reasons": sorted(self.reasons), "samples": len(mhz)}
+        if len(self.marks) >= 2:  # the samples inside the timed window, and the warm-up window before it
+            a, b = self.marks[0], self.marks[1]
+            inside = [v for t, v in self.samples if a <= t <= b]
+            before = [v for t, v in self.samples if t < a]
+            out["timed_window"] = {"sm_mhz": statistics.median(inside) if inside else None, "samples": len(inside),
+                                   "ms": round((b - a) * 1e3, 3)}
+            out["warmup_window"] = {"sm_mhz": statistics.median(before) if before else None, "samples": len(before)}
+            if inside:
+                out["sm_mhz"] = statistics.median(inside)
+        return out
 
 
 def nvml_index(dev) -> int:
@@ -192,11 +208,23 @@ def reference_gpu_kernel() -> dict | None:
                              tab.ctypes.data, c.ctypes.data, 100)
     if ms <= 0:
         return None
-    return {"value": round(BYTES_PER_STATE * m.n_states / (ms * 1e-3) / 1e9, 3), "unit": "GB/s",
-            "ms_per_action": round(ms, 4),
-            "kernel": "reference fspmat_sdkron_mv built for sm_100a, called through SDKronMatSet::action "
-                      "(coefficient copy and device synchronisation per call, as the reference does); "
-                      "100 actions (the count of the reference's benchmark_fsp_mat.cu:158), CUDA events, x and y resident"}
+    out = {"value": round(BYTES_PER_STATE * m.n_states / (ms * 1e-3) / 1e9, 3), "unit": "GB/s",
+           "ms_per_action": round(ms, 4),
+           "kernel": "reference fspmat_sdkron_mv built for sm_100a, called through SDKronMatSet::action "
+                     "(coefficient copy and device synchronisation per call, as the reference does); "
+                     "100 actions (the count of the reference's benchmark_fsp_mat.cu:158), CUDA events, x and y resident"}
+    # The reference's HYB format (src/fspmat_hyb_kernels.cu:66-106) on the same workload, built by its
+    # own fill kernel from a factor-table PropFun; GB/s counted with the sparse format's algorithmic
+    # bytes (x, y and one propensity table row per reaction: 24 + 8 nr B/state), as our sparse leg is.
+    import ctypes as C
+    hms = C.c_double(0.0)
+    rc = R.ref_gpu_hyb_tables(m.ns, m.nr, b.ctypes.data, sv.ctypes.data, sc.ctypes.data, sr.ctypes.data,
+                              tab.ctypes.data, c.ctypes.data, None, None, 100, C.addressof(hms))
+    if rc == 0 and hms.value > 0:
+        out["hyb"] = {"value": round((24 + 8 * m.nr) * m.n_states / (hms.value * 1e-3) / 1e9, 3), "unit": "GB/s",
+                      "ms_per_action": round(hms.value, 4), "bytes_per_state": 24 + 8 * m.nr,
+                      "kernel": "reference fspmat_hyb_mv built for sm_100a through HYBMatSet::action, 100 actions"}
+    return out
 
 
 def run_reference(args):
@@ -489,25 +517,29 @@ def run_ours(args):
 
     for i in range(max(3, args.warmup)):
         step(i)
-    # keep warming up (untimed) for ~0.5 s so the SM clock has left its idle state
+    # Warm-up beyond the W steps: ~30 ms of launches, so the SM clock has left its idle state.  The
+    # timed region is then a burst of K launches (the regime of the HBM copy peak it is compared
+    # with); the same launches over ~1 s, under the power cap, are reported beside it as `sustained`.
+    clocks = ClockSampler(nvml_index(dev))
+    clocks.start()
     t_w = time.perf_counter()
     i = 0
-    while not args.no_extras and time.perf_counter() - t_w < 0.5:
-        for _ in range(50):
+    while not args.no_extras and time.perf_counter() - t_w < 0.03:
+        for _ in range(20):
             step(i)
             i += 1
         torch.cuda.synchronize(dev)
     if world > 1:
         dist.barrier()
-    clocks = ClockSampler(nvml_index(dev))
-    clocks.start()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize(dev)
+    clocks.mark()
     ev0.record(stream)
     for i in range(args.steps):
         step(i)
     ev1.record(stream)
     torch.cuda.synchronize(dev)
+    clocks.mark()
     ms = ev0.elapsed_time(ev1) / args.steps
     if world > 1:
         t = torch.tensor([ms], device=dev)
@@ -515,6 +547,24 @@ def run_ours(args):
         ms = t.item()
         dist.barrier()
     clk = clocks.stop()
+    sustained = None
+    if not args.no_extras:  # the same launches over ~1 s (power-capped regime), reported beside
+        k_s = max(args.steps, int(1.0 / max(ms * 1e-3, 1e-6)))
+        cs = ClockSampler(nvml_index(dev))
+        cs.start()
+        torch.cuda.synchronize(dev)
+        ev0.record(stream)
+        for i in range(k_s):
+            step(i)
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+        ms_s = ev0.elapsed_time(ev1) / k_s
+        if world > 1:
+            t = torch.tensor([ms_s], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms_s = t.item()
+        sustained = {"value": round(BYTES_PER_STATE * n / (ms_s * 1e-3) / 1e9 * world, 3), "unit": "GB/s",
+                     "ms_per_step": round(ms_s, 5), "steps": k_s, "clocks": cs.stop()}
     kernel_gbs = BYTES_PER_STATE * n / (ms * 1e-3) / 1e9
     value = kernel_gbs * world
     if args.no_extras:  # profiling runs: the timed generator action only
@@ -575,6 +625,7 @@ def run_ours(args):
             "cpu_baseline": ({k: (round(v, 3) if isinstance(v, float) else v) for k, v in cpu.items() if k != "ms_per_step"}
                              if cpu else None),
             "clocks": clk,
+            "sustained": sustained,
             "gpu_launches": args.steps,
             "secondary": secondary,
         }

@@ -155,6 +155,8 @@ SIGNATURES = {
     "cufsp_solver_solve": [_P, _P, _P, C.POINTER(SolverStatus)],
     "cufsp_solver_reset_time": [_P],
     "cufsp_loglik": [C.c_int64, _P, C.c_int64, _P, _DP, _P],
+    "cufsp_likelihood_eval": [_P, _DP, C.c_int, _DP, _P, C.c_int64, _P, C.c_int, C.c_double, _DP, _DP, _P],
+    "cufsp_mat_create_table": [C.POINTER(ModelDesc), C.c_int, _DP, C.POINTER(_P)],
     "cufsp_likelihood_grad": [_P, _DP, C.c_int, _DP, _P, C.c_int64, _P, C.c_int, C.c_double, _DP, _DP, _P],
     "cufsp_likelihood_grad_batched": [C.POINTER(ModelDesc), C.c_int, _DP, C.c_int, _DP, _P, C.c_int64, _P, C.c_int,
                                       C.c_double, C.c_int, _DP, _DP],

@@ -28,13 +28,15 @@ NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-rdc=true", "-Xcompiler"
                      "-I" + str(ROOT / "include"), "--expt-relaxed-constexpr", "--extended-lambda"]
 # The small dense kernels of the host Pade exponential vectorise at -O3 only.
 HOST_EXTRA = {"cufsp_expm.cpp": ["-Xcompiler", "-O3"]}
-SOURCES = ["cufsp_common.cu", "cufsp_kron.cu", "cufsp_kron_plane.cu", "cufsp_kron_march.cu", "cufsp_sparse.cu", "cufsp_mat.cu",
+SOURCES = ["cufsp_common.cu", "cufsp_rtc.cu", "cufsp_kron.cu", "cufsp_kron_plane.cu", "cufsp_kron_march.cu", "cufsp_sparse.cu", "cufsp_mat.cu",
            "cufsp_krylov.cu", "cufsp_expm.cpp", "cufsp_noalloc.cu", "cufsp_stats.cu", "cufsp_solver.cu",
            "cufsp_vec.cu", "cufsp_bdf.cu", "cufsp_batch.cu", "cufsp_adjoint.cu", "cufsp_adaptive.cu",
            "cufsp_arnoldi.cu"]
-HEADERS = ["cufsp_internal.h", "cufsp_reduce.cuh", "cufsp_march.h", "cufsp_vec.h", "cufsp_plane.cuh", "cufsp_batch.cuh"]
+HEADERS = ["cufsp_internal.h", "cufsp_reduce.cuh", "cufsp_march.h", "cufsp_vec.h", "cufsp_plane.cuh", "cufsp_batch.cuh",
+           "cufsp_sparse_rtc.cuh"]
 # Kernel sources compiled at run time by NVRTC are embedded in the library as string literals.
-RTC_SOURCES = {"cufsp_plane.cuh": "cufsp_plane_src.inc", "cufsp_batch.cuh": "cufsp_batch_src.inc"}
+RTC_SOURCES = {"cufsp_plane.cuh": "cufsp_plane_src.inc", "cufsp_batch.cuh": "cufsp_batch_src.inc",
+               "cufsp_sparse_rtc.cuh": "cufsp_sparse_src.inc"}
 LINK_LIBS = ["-L/usr/local/cuda/lib64", "-lnvrtc", "-Xlinker", "-rpath,/usr/local/cuda/lib64"]
 
 
@@ -72,7 +74,7 @@ def _embed_rtc_sources(force: bool) -> None:
 
 
 def _compile(src: Path, obj: Path, extra: list[str], force: bool) -> Path:
-    deps = [src] + [CSRC / h for h in HEADERS] + [ROOT / "include" / "cufsp.h"]
+    deps = [src] + [CSRC / h for h in HEADERS] + [ROOT / "include" / "cufsp.h", ROOT / "include" / "cufsp.hpp"]
     deps += [OBJ / inc for inc in RTC_SOURCES.values()]
     if force or _stale(obj, deps):
         obj.parent.mkdir(parents=True, exist_ok=True)

@@ -380,7 +380,7 @@ cufsp_status launch_scale(int64_t n, double *x, const double *d_alpha, double al
 
 // ---- model validation -------------------------------------------------------------------------
 
-cufsp_status model_from_desc(const cufsp_model_desc *d, bool need_tables, ModelHost &m) {
+cufsp_status model_from_desc(const cufsp_model_desc *d, bool need_tables, ModelHost &m, bool external_table) {
     if (!d) return set_error(CUFSP_ERR_INVALID_ARG, "model descriptor is NULL");
     if (d->n_species < 1 || d->n_species > CUFSP_MAX_SPECIES)
         return set_error(CUFSP_ERR_INVALID_ARG, "n_species must be in [1, 16]");
@@ -435,7 +435,7 @@ cufsp_status model_from_desc(const cufsp_model_desc *d, bool need_tables, ModelH
         if (!std::isfinite(v)) return set_error(CUFSP_ERR_NONFINITE, "propensity factor table holds NaN/Inf");
     if (need_tables && m.tables.empty())
         return set_error(CUFSP_ERR_INVALID_ARG, "KRONECKER format needs factor_tables or prop_factor");
-    if (m.tables.empty() && !m.prop_device)
+    if (m.tables.empty() && !m.prop_device && !external_table)
         return set_error(CUFSP_ERR_INVALID_ARG, "no propensity source (factor_tables, prop_factor or prop_device)");
     return CUFSP_SUCCESS;
 }

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -105,13 +106,15 @@ struct ModelHost {
     std::vector<int> bounds;       // b_s
     std::vector<int> nu;           // dense stoichiometry [nr][ns]
     std::vector<double> tables;    // [nr][sum_s(b_s+1)] or empty
+    std::vector<double> prop_table;  // [nr][n] propensities evaluated by the caller (sparse formats) or empty
     std::vector<int> tab_off;      // [ns] offset of species s inside a reaction's block
     int tab_stride = 0;            // sum_s (b_s + 1)
     cufsp_prop_fn prop_device = nullptr;
     cufsp_tcoef_fn tcoef = nullptr;
     void *tcoef_user = nullptr;
 };
-cufsp_status model_from_desc(const cufsp_model_desc *d, bool need_tables, ModelHost &m);
+// external_table: the propensities come from a caller-evaluated table (cufsp_mat_create_table).
+cufsp_status model_from_desc(const cufsp_model_desc *d, bool need_tables, ModelHost &m, bool external_table = false);
 
 // ---- format back-ends ----------------------------------------------------------------------
 struct KronData;    // matrix-free factorised generator (cufsp_kron.cu)
@@ -139,6 +142,17 @@ cufsp_status sparse_apply(SparseData *s, const double *coefs, double alpha, cons
                           int64_t i_begin = 0, int64_t i_end = -1);
 cufsp_status sparse_export(const SparseData *s, double *d_props, cudaStream_t st);
 int64_t sparse_halo(const SparseData *s);
+const std::string &sparse_describe(const SparseData *s);
+
+// Kernels compiled at run time by NVRTC for sm_100a (cufsp_rtc.cu): cached per process by source
+// text; nullptr with the reason in `why` when compiling or loading fails.
+struct RtcModule {
+    cudaLibrary_t lib = nullptr;
+    std::vector<cudaKernel_t> kernels;  // in the order of the requested names
+    std::string log;
+};
+std::shared_ptr<RtcModule> rtc_module(const std::string &src, const std::vector<std::string> &names,
+                                      std::string &why);
 
 // Runtime-specialised plane kernel for near-neighbour networks of 2-3 species (cufsp_kron_plane.cu).
 struct PlaneData;

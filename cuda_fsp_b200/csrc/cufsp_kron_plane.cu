@@ -8,8 +8,6 @@
 // cudaLibraryLoadData.  Compiled kernels are cached per process by their full source text, so
 // generators of the same network over other boxes reuse them.  Networks of other shapes, and
 // applies over a range that is not whole planes, use k_kron_mv (cufsp_kron.cu).
-#include <nvrtc.h>
-
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
@@ -29,65 +27,9 @@ const char *kPlaneSource =
 #include "cufsp_plane_src.inc"
     ;
 
-struct PlaneKernels {
-    cudaLibrary_t lib = nullptr;
-    cudaKernel_t accum = nullptr, set = nullptr;
-    std::string log;
-};
-
-std::mutex g_plane_mu;
-std::map<std::string, std::shared_ptr<PlaneKernels>> g_plane_cache;
-
 int env_int(const char *name, int dflt) {
     const char *v = getenv(name);
     return v ? atoi(v) : dflt;
-}
-
-// Compile (or fetch) the kernels for one generated source; nullptr with `why` set on failure.
-std::shared_ptr<PlaneKernels> plane_kernels(const std::string &src, std::string &why) {
-    std::lock_guard<std::mutex> lock(g_plane_mu);
-    auto it = g_plane_cache.find(src);
-    if (it != g_plane_cache.end()) return it->second;
-    auto pk = std::make_shared<PlaneKernels>();
-    nvrtcProgram prog;
-    if (nvrtcCreateProgram(&prog, src.c_str(), "cufsp_plane.cu", 0, nullptr, nullptr) != NVRTC_SUCCESS) {
-        why = "nvrtcCreateProgram failed";
-        return nullptr;
-    }
-    const char *opts[] = {"--gpu-architecture=sm_100a", "-std=c++17", "--fmad=true", "-lineinfo"};
-    const nvrtcResult rc = nvrtcCompileProgram(prog, 4, opts);
-    size_t log_size = 0;
-    nvrtcGetProgramLogSize(prog, &log_size);
-    if (log_size > 1) {
-        pk->log.resize(log_size);
-        nvrtcGetProgramLog(prog, &pk->log[0]);
-    }
-    if (rc != NVRTC_SUCCESS) {
-        why = std::string("NVRTC: ") + nvrtcGetErrorString(rc) + ": " + pk->log.substr(0, 2000);
-        nvrtcDestroyProgram(&prog);
-        return nullptr;
-    }
-    size_t cubin_size = 0;
-    std::vector<char> cubin;
-    if (nvrtcGetCUBINSize(prog, &cubin_size) == NVRTC_SUCCESS && cubin_size > 0) {
-        cubin.resize(cubin_size);
-        if (nvrtcGetCUBIN(prog, cubin.data()) != NVRTC_SUCCESS) cubin.clear();
-    }
-    nvrtcDestroyProgram(&prog);
-    if (cubin.empty()) {
-        why = "NVRTC produced no cubin";
-        return nullptr;
-    }
-    cudaError_t e = cudaLibraryLoadData(&pk->lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0);
-    if (e == cudaSuccess) e = cudaLibraryGetKernel(&pk->accum, pk->lib, "cufsp_plane_mv_accum");
-    if (e == cudaSuccess) e = cudaLibraryGetKernel(&pk->set, pk->lib, "cufsp_plane_mv_set");
-    if (e != cudaSuccess) {
-        why = std::string("loading the plane kernel: ") + cudaGetErrorString(e);
-        cudaGetLastError();
-        return nullptr;
-    }
-    g_plane_cache[src] = pk;
-    return pk;
 }
 
 void emit_fn(std::ostringstream &s, const char *name, const std::vector<int> &v) {
@@ -126,7 +68,7 @@ __global__ void k_plane_words(const WordArgs a, const double2 *__restrict__ gtab
 }
 
 struct PlaneData {
-    std::shared_ptr<PlaneKernels> k;
+    std::shared_ptr<RtcModule> k;  // kernels[0] accumulate form, kernels[1] overwrite form
     int n0 = 0, n1 = 1, n2 = 0, nr = 0, tr = 1;
     int row_blocks = 0, threads = 0, pitch = 0;
     size_t smem_accum = 0, smem_set = 0;
@@ -324,18 +266,14 @@ PlaneData *plane_create(const ModelHost &m, const double *d_tables, std::string 
     emit_fn(s, "dg_fb", dg_fb);
     s << "}\n";
     const std::string src = s.str() + kPlaneSource;
-    pd->k = plane_kernels(src, why);
+    pd->k = rtc_module(src, {"cufsp_plane_mv_accum", "cufsp_plane_mv_set"}, why);
     if (!pd->k) return nullptr;
-    cudaError_t e = cudaFuncSetAttribute((const void *)pd->k->accum, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)pd->smem_accum);
+    const void *k_accum = (const void *)pd->k->kernels[0], *k_set = (const void *)pd->k->kernels[1];
+    cudaError_t e = cudaFuncSetAttribute(k_accum, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pd->smem_accum);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_set, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pd->smem_set);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute((const void *)pd->k->set, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pd->smem_set);
-    if (e == cudaSuccess)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pd->occ_accum, (const void *)pd->k->accum, pd->threads,
-                                                          pd->smem_accum);
-    if (e == cudaSuccess)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pd->occ_set, (const void *)pd->k->set, pd->threads,
-                                                          pd->smem_set);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pd->occ_accum, k_accum, pd->threads, pd->smem_accum);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pd->occ_set, k_set, pd->threads, pd->smem_set);
     if (e != cudaSuccess || pd->occ_accum < 1 || pd->occ_set < 1) {
         cudaGetLastError();
         why = "plane kernel does not fit an SM";
@@ -472,7 +410,7 @@ bool plane_launch(PlaneData *pd, const double *coefs, double alpha, const double
     const int segs = (planes + a.zseg - 1) / a.zseg;
     a.items = pd->row_blocks * segs;
     void *args[] = {&a, (void *)&x, (void *)&y};
-    cudaError_t e = cudaLaunchKernel((const void *)(accumulate ? pd->k->accum : pd->k->set), dim3((unsigned)a.items),
+    cudaError_t e = cudaLaunchKernel((const void *)pd->k->kernels[accumulate ? 0 : 1], dim3((unsigned)a.items),
                                      dim3((unsigned)pd->threads), args, accumulate ? pd->smem_accum : pd->smem_set, st);
     if (e != cudaSuccess) *status = cuda_error(e, "plane kernel launch");
     return true;

@@ -67,6 +67,48 @@ extern "C" cufsp_status cufsp_mat_create(const cufsp_model_desc *desc, cufsp_for
     return CUFSP_SUCCESS;
 }
 
+// Sparse-format generator from propensities the caller evaluated on the host, for models whose
+// propensity is host code (the legacy cme::Model::propensity, src/Model.h:14-26) rather than a device
+// PropFun or factor tables: prop_table[r * n + i] = a_r(x_i), n = number of states.
+extern "C" cufsp_status cufsp_mat_create_table(const cufsp_model_desc *desc, cufsp_format format,
+                                               const double *prop_table, cufsp_mat **out) {
+    clear_error();
+    if (!out || !desc || !prop_table) return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_mat_create_table: NULL argument");
+    *out = nullptr;
+    if (format != CUFSP_FORMAT_CSR && format != CUFSP_FORMAT_HYB)
+        return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_mat_create_table: a propensity table makes a CSR or HYB generator");
+    cufsp_model_desc d = *desc;  // the table is the propensity source: the descriptor's own are ignored
+    d.factor_tables = nullptr;
+    d.prop_factor = nullptr;
+    d.prop_device = nullptr;
+    cufsp_mat *A = new cufsp_mat();
+    A->format = format;
+    cufsp_status s = model_from_desc(&d, false, A->model, /*external_table=*/true);
+    if (s == CUFSP_SUCCESS) {
+        const size_t cnt = (size_t)A->model.nr * (size_t)A->model.n;
+        A->model.prop_table.assign(prop_table, prop_table + cnt);
+        for (double v : A->model.prop_table)
+            if (!std::isfinite(v)) {
+                s = set_error(CUFSP_ERR_NONFINITE, "cufsp_mat_create_table: propensity table holds NaN/Inf");
+                break;
+            }
+    }
+    if (s == CUFSP_SUCCESS) {
+        int dev_count = 0;
+        const cudaError_t e = cudaGetDeviceCount(&dev_count);
+        if (e != cudaSuccess || dev_count == 0) s = set_error(CUFSP_ERR_NO_DEVICE, "no CUDA device available");
+    }
+    if (s == CUFSP_SUCCESS) s = sparse_create(A->model, &A->sparse);
+    A->model.prop_table.clear();
+    A->model.prop_table.shrink_to_fit();
+    if (s != CUFSP_SUCCESS) {
+        cufsp_mat_destroy(A);
+        return s;
+    }
+    *out = A;
+    return CUFSP_SUCCESS;
+}
+
 extern "C" cufsp_status cufsp_mat_destroy(cufsp_mat *A) {
     if (!A) return CUFSP_SUCCESS;
     if (A->kron) kron_destroy(A->kron);
@@ -129,7 +171,7 @@ cufsp_status mat_check_watchdog(cufsp_mat *A, const char *where) {
 
 extern "C" cufsp_status cufsp_mat_describe(const cufsp_mat *A, char *buf, size_t len) {
     if (!A || !buf || len == 0) return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_mat_describe: bad argument");
-    const std::string d = A->kron ? "KRONECKER: " + kron_describe(A->kron) : std::string("sparse: k_sparse_mv");
+    const std::string d = A->kron ? "KRONECKER: " + kron_describe(A->kron) : sparse_describe(A->sparse);
     const size_t k = std::min(len - 1, d.size());
     std::memcpy(buf, d.data(), k);
     buf[k] = 0;

@@ -15,10 +15,21 @@
 // tables, multiplied in species order ((1 * f_0) * f_1) * ...
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <sstream>
 
 #include "cufsp_internal.h"
+#define CUFSP_SPARSE_RTC_MAX_R 64
+#include "cufsp_sparse_rtc.cuh"
 
 namespace cufsp {
+
+namespace {
+const char *kSparseSource =
+#include "cufsp_sparse_src.inc"
+    ;
+}  // namespace
 
 struct SparseArgs {
     const double *__restrict__ P;       // [nr][n]
@@ -131,7 +142,78 @@ struct SparseData {
     std::vector<int> bounds;
     int64_t halo = 0;
     int grid_full = 0;
+    // kernel specialised for this network and box (cufsp_sparse_rtc.cuh); null: k_sparse_mv
+    std::shared_ptr<RtcModule> rtc;
+    int rtc_grid = 0;
+    std::string describe;
 };
+
+namespace {
+
+// Compiles the specialised kernel for this network and box; sets sd->rtc or the reason in `why`.
+void sparse_build_rtc(const ModelHost &m, SparseData *sd, std::string &why) {
+    const char *ev = getenv("CUFSP_SPARSE_RTC");
+    if (ev && atoi(ev) == 0) {
+        why = "disabled (CUFSP_SPARSE_RTC=0)";
+        return;
+    }
+    if (m.nr > CUFSP_SPARSE_RTC_MAX_R) {
+        why = "more than 64 reactions";
+        return;
+    }
+    if (m.n % 2 != 0) {  // table rows of 16-byte pairs need an even row length
+        why = "odd number of states";
+        return;
+    }
+    std::vector<int64_t> stride(m.ns);
+    int64_t st = 1;
+    for (int s = 0; s < m.ns; ++s) {
+        stride[s] = st;
+        st *= (int64_t)m.bounds[s] + 1;
+    }
+    // reactions whose loads are in flight together, and CTAs per SM the launch bounds promise
+    // (CUFSP_SPARSE_CHUNK / CUFSP_SPARSE_MINB override them for tuning)
+    const char *ec = getenv("CUFSP_SPARSE_CHUNK");
+    const char *em = getenv("CUFSP_SPARSE_MINB");
+    const int chunk = std::max(1, std::min(m.nr, ec ? atoi(ec) : (m.nr <= 12 ? m.nr : 8)));
+    const int minb = std::max(1, std::min(8, em ? atoi(em) : 1));
+    std::ostringstream o;
+    o << "#define CUFSP_SPARSE_MINB " << minb << "\n";
+    o << "#define CUFSP_SPARSE_RTC_MAX_R " << CUFSP_SPARSE_RTC_MAX_R << "\n#define CUFSP_SPARSE_NS " << m.ns
+      << "\n#define CUFSP_SPARSE_NR " << m.nr << "\n#define CUFSP_SPARSE_N " << m.n << "LL\n#define CUFSP_SPARSE_CHUNK "
+      << chunk << "\nnamespace cufsp_sparse {\n";
+    o << "__device__ __forceinline__ constexpr int ext(int s) {";
+    for (int s = 0; s < m.ns; ++s) o << " if (s == " << s << ") return " << m.bounds[s] + 1 << ";";
+    o << " return 1; }\n";
+    o << "__device__ __forceinline__ constexpr int nu(int r, int s) {";
+    for (int r = 0; r < m.nr; ++r)
+        for (int s = 0; s < m.ns; ++s) {
+            const int v = m.nu[(size_t)r * m.ns + s];
+            if (v != 0) o << " if (r == " << r << " && s == " << s << ") return " << v << ";";
+        }
+    o << " return 0; }\n";
+    o << "__device__ __forceinline__ constexpr bool touches(int r, int s) { return nu(r, s) != 0; }\n";
+    o << "__device__ __forceinline__ constexpr long long shift(int r) {";
+    for (int r = 0; r < m.nr; ++r) {
+        int64_t d = 0;
+        for (int s = 0; s < m.ns; ++s) d += (int64_t)m.nu[(size_t)r * m.ns + s] * stride[s];
+        o << " if (r == " << r << ") return " << d << "LL;";
+    }
+    o << " return 0; }\n}\n";
+    sd->rtc = rtc_module(o.str() + kSparseSource, {"cufsp_sparse_mv_accum", "cufsp_sparse_mv_set"}, why);
+    if (!sd->rtc) return;
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, (const void *)sd->rtc->kernels[0], 256, 0) != cudaSuccess ||
+        occ < 1) {
+        cudaGetLastError();
+        sd->rtc.reset();
+        why = "specialised kernel does not fit an SM";
+        return;
+    }
+    sd->rtc_grid = device_info().sm_count * occ;
+}
+
+}  // namespace
 
 cufsp_status sparse_create(const ModelHost &m, SparseData **out) {
     SparseData *sd = new SparseData();
@@ -167,12 +249,15 @@ cufsp_status sparse_create(const ModelHost &m, SparseData **out) {
     if (e == cudaSuccess) e = dev_malloc(&sd->d_rinfo, sizeof(int) * rinfo.size());
     if (e == cudaSuccess) e = cudaMemcpy(sd->d_rinfo, rinfo.data(), sizeof(int) * rinfo.size(), cudaMemcpyHostToDevice);
     double *d_tables = nullptr;
-    if (e == cudaSuccess && !m.prop_device) {
+    if (e == cudaSuccess && !m.prop_table.empty()) {  // table evaluated by the caller on the host
+        e = cudaMemcpy(sd->d_P, m.prop_table.data(), sizeof(double) * (size_t)m.nr * (size_t)m.n,
+                       cudaMemcpyHostToDevice);
+    } else if (e == cudaSuccess && !m.prop_device) {
         e = dev_malloc(&d_tables, sizeof(double) * m.tables.size());
         if (e == cudaSuccess)
             e = cudaMemcpy(d_tables, m.tables.data(), sizeof(double) * m.tables.size(), cudaMemcpyHostToDevice);
     }
-    if (e == cudaSuccess) {
+    if (e == cudaSuccess && m.prop_table.empty()) {
         FillArgs f;
         f.tables = d_tables;
         f.prop = m.prop_device;
@@ -195,9 +280,16 @@ cufsp_status sparse_create(const ModelHost &m, SparseData **out) {
         return cuda_error(e, "sparse_create");
     }
     // P must be finite for the action to be well defined.
+    std::string why;
+    sparse_build_rtc(m, sd, why);
+    sd->describe = sd->rtc ? "sparse: propensity table, kernel specialised for the network and box (NVRTC, sm_100a), " +
+                                 std::to_string(sd->rtc_grid) + " CTAs x 256 threads"
+                           : "sparse: propensity table, k_sparse_mv (" + why + ")";
     *out = sd;
     return CUFSP_SUCCESS;
 }
+
+const std::string &sparse_describe(const SparseData *s) { return s->describe; }
 
 void sparse_destroy(SparseData *s) {
     if (!s) return;
@@ -236,6 +328,22 @@ cufsp_status sparse_apply(SparseData *sd, const double *coefs, double alpha, con
     for (int r = 0; r < CUFSP_MAX_REACTIONS_SPARSE; ++r) a.coef[r] = r < sd->nr ? alpha * coefs[r] : 0.0;
     const int64_t cnt = i_end - i_begin;
     if (cnt <= 0) return CUFSP_SUCCESS;
+    if (sd->rtc && ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) % 16) == 0) {
+        CufspSparseRtcArgs r;
+        std::memset(&r, 0, sizeof(r));
+        r.P = sd->d_P;
+        r.d_alpha = d_alpha;
+        r.d_skip = d_skip;
+        r.i_begin = i_begin;
+        r.i_end = i_end;
+        for (int k = 0; k < sd->nr; ++k) r.coef[k] = alpha * coefs[k];
+        const int64_t pairs = (i_end - (i_begin & ~(int64_t)1) + 1) / 2;
+        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(sd->rtc_grid, (pairs + 255) / 256));
+        void *args[] = {&r, (void *)&x, (void *)&y};
+        CUFSP_CUDA_TRY(cudaLaunchKernel((const void *)sd->rtc->kernels[accumulate ? 0 : 1], dim3(grid), dim3(256), args,
+                                        0, st));
+        return CUFSP_SUCCESS;
+    }
     const int grid = stream_grid(cnt, 2, sd->grid_full);
     const size_t smem = sizeof(int) * (size_t)sd->nr * (2 + sd->ns);
     SparseKernel k = sd->ns <= 2 ? pick_sparse_acc<2>(accumulate)

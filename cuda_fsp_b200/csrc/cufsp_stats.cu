@@ -9,6 +9,7 @@
 #include <curand_kernel.h>
 
 #include <cmath>
+#include <vector>
 
 #include "cufsp_internal.h"
 #include "cufsp_reduce.cuh"
@@ -124,6 +125,75 @@ extern "C" cufsp_status cufsp_loglik(int64_t n, const double *d_p, int64_t block
     }
     if (d_out) cudaFree(d_out);
     rs.release();
+    return s;
+}
+
+// Likelihood::evaluate (src/Likelihood.cpp:8-33) as one call: the Krylov solve carries p(0) through
+// the data times and every time's term is reduced on the device into its own slot; one device->host
+// read at the end.  The solve is KryExpvFSP::solve between consecutive times (t_now carries over).
+extern "C" cufsp_status cufsp_likelihood_eval(cufsp_mat *A, const double *coefs, int n_times, const double *times,
+                                              const double *d_p0, int64_t block, const double *d_counts, int m,
+                                              double tol, double *logL, double *fsp_error, cufsp_stream_t stream) {
+    clear_error();
+    if (!A || !times || !d_p0 || !d_counts || !logL || n_times < 1)
+        return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_likelihood_eval: NULL argument");
+    int64_t n = 0;
+    cufsp_mat_num_states(A, &n);
+    if (block < 1 || n % block != 0 || block > 2147483647LL)
+        return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_likelihood_eval: bad block");
+    for (int i = 0; i < n_times; ++i)
+        if (!(times[i] >= (i ? times[i - 1] : 0.0)) || !std::isfinite(times[i]))
+            return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_likelihood_eval: times must be finite and non-decreasing");
+    cudaStream_t st = (cudaStream_t)stream;
+    cufsp_expv *E = nullptr;
+    cufsp_status s = cufsp_expv_create(n, m, tol, 0, 2, 1.0, &E);
+    if (s == CUFSP_SUCCESS) {
+        if (coefs) s = cufsp_expv_bind_mat_coefs(E, A, coefs);
+        else s = cufsp_expv_bind_mat(E, A, 0.0);
+    }
+    double *p = nullptr, *d_ll = nullptr;
+    ReduceScratch rs;
+    const int ctas = device_info().sm_count * 4;
+    if (s == CUFSP_SUCCESS && cache_alloc((void **)&p, sizeof(double) * (size_t)n) != cudaSuccess)
+        s = set_error(CUFSP_ERR_ALLOC, "cufsp_likelihood_eval: device allocation failed");
+    if (s == CUFSP_SUCCESS && cache_alloc((void **)&d_ll, sizeof(double) * (size_t)(n_times + 2)) != cudaSuccess)
+        s = set_error(CUFSP_ERR_ALLOC, "cufsp_likelihood_eval: device allocation failed");
+    if (s == CUFSP_SUCCESS) s = rs.init(ctas, 1);
+    if (s == CUFSP_SUCCESS) {
+        const cudaError_t e = cudaMemcpyAsync(p, d_p0, sizeof(double) * (size_t)n, cudaMemcpyDeviceToDevice, st);
+        if (e != cudaSuccess) s = cuda_error(e, "cufsp_likelihood_eval");
+    }
+    // mass at t = 0 (for the FSP error)
+    if (s == CUFSP_SUCCESS) s = launch_sum(n, p, d_ll + n_times, rs, st);
+    const int64_t nk = n / block;
+    for (int i = 0; i < n_times && s == CUFSP_SUCCESS; ++i) {
+        s = cufsp_expv_set_final_time(E, times[i]);
+        if (s == CUFSP_SUCCESS) s = cufsp_expv_solve(E, p, stream, nullptr);
+        if (s != CUFSP_SUCCESS) break;
+        const int g = stream_grid(nk, 1, ctas);
+        k_loglik<<<g, kRedThreads, 0, st>>>(nk, (int)block, p, d_counts + (size_t)i * nk, rs.partials, rs.counter,
+                                            d_ll + i);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) s = cuda_error(e, "cufsp_likelihood_eval");
+    }
+    if (s == CUFSP_SUCCESS) s = launch_sum(n, p, d_ll + n_times + 1, rs, st);
+    std::vector<double> h(n_times + 2, 0.0);
+    if (s == CUFSP_SUCCESS) {
+        cudaError_t e = cudaMemcpyAsync(h.data(), d_ll, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) s = cuda_error(e, "cufsp_likelihood_eval");
+    }
+    if (s == CUFSP_SUCCESS) {
+        double ll = 0.0;
+        for (int i = 0; i < n_times; ++i) ll += h[i];  // time order, as the reference's loop
+        *logL = ll;
+        if (fsp_error) *fsp_error = h[n_times] - h[n_times + 1];
+    }
+    cudaStreamSynchronize(st);
+    cufsp_expv_destroy(E);
+    cache_free(p, st);
+    cache_free(d_ll, st);
+    rs.release(st);
     return s;
 }
 

@@ -201,20 +201,25 @@ class Likelihood:
         return ll + float(np.sum(self.outside)) * math.log(1e-44), g
 
     def evaluate(self, coefs=None) -> float:
+        """log L at coefs (default: the last coefficients given, initially the model's rates) in one
+        call of cufsp_likelihood_eval: the Krylov solve from p0 through the data times and every time's
+        term reduced on the device (Likelihood::evaluate, src/Likelihood.cpp:8-33).  The FSP error at
+        the last time is kept in fsp_errors."""
         if coefs is not None:
             self.solver.set_coefs(coefs)
-        self.p.copy_(self.p0)  # return the distribution to the initial condition (:24-30)
-        self.solver.reset_time()
-        lib, n = self.A._lib, self.model.n_states
-        ll, self.fsp_errors = 0.0, []
-        for it in range(len(self.times)):
-            st = self.solver.next_time()
-            self.fsp_errors.append(st["fsp_error"])
-            out = C.c_double()
-            _lib.check(lib, lib.cufsp_loglik(n, self.p.data_ptr(), self.block, self.counts[it].data_ptr(),
-                                             C.byref(out), _stream(None)), "cufsp_loglik")
-            ll += out.value + self.outside[it] * math.log(1e-44)
-        return ll
+            self._coefs = np.ascontiguousarray(np.asarray(coefs, np.float64))
+        c = getattr(self, "_coefs", None)
+        if c is None:
+            c = self._coefs = np.ascontiguousarray(self.model.coefs(0.0))
+        t = np.ascontiguousarray(self.times)
+        lib = self.A._lib
+        ll, err = C.c_double(), C.c_double()
+        dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))  # noqa: E731
+        _lib.check(lib, lib.cufsp_likelihood_eval(
+            self.A.handle, dp(c), len(t), dp(t), self.p0.data_ptr(), self.block, self.counts.data_ptr(), int(self.m),
+            float(self.kry_tol), C.byref(ll), C.byref(err), _stream(None)), "cufsp_likelihood_eval")
+        self.fsp_errors = [err.value]
+        return ll.value + float(np.sum(self.outside)) * math.log(1e-44)
 
 
 class AdaptiveFSP:

@@ -98,6 +98,12 @@ cufsp_status cufsp_get_states(int n_species, const int *fsp_bounds, int *d_state
  * src/FSPMat.cu:49-76 with PropFactorFun).  Synchronises the device once (assembly). */
 cufsp_status cufsp_mat_create(const cufsp_model_desc *desc, cufsp_format format, cufsp_mat **out);
 cufsp_status cufsp_mat_destroy(cufsp_mat *A);
+/* CSR/HYB generator from propensities evaluated by the caller on the host: prop_table[r * n + i] =
+ * a_r(x_i) (host, n_reactions * n_states doubles, copied).  For models whose propensity is host code
+ * -- the legacy cme::Model::propensity (src/Model.h:14-26), a host function of the state -- rather than
+ * a device PropFun or factor tables.  The descriptor's propensity fields are ignored.  Synchronises. */
+cufsp_status cufsp_mat_create_table(const cufsp_model_desc *desc, cufsp_format format, const double *prop_table,
+                                    cufsp_mat **out);
 /* get_n_rows / get_n_species / get_n_reactions, src/FSPMat.cu:108-118 */
 cufsp_status cufsp_mat_num_states(const cufsp_mat *A, int64_t *n_states);
 cufsp_status cufsp_mat_dims(const cufsp_mat *A, int *n_species, int *n_reactions, cufsp_format *format);
@@ -280,6 +286,15 @@ cufsp_status cufsp_adaptive_solution(const cufsp_adaptive *S, const double **d_p
  * (block = 1: no marginalisation).  d_p, d_counts: device, n and n/block doubles.  Synchronous. */
 cufsp_status cufsp_loglik(int64_t n, const double *d_p, int64_t block, const double *d_counts, double *out,
                           cufsp_stream_t stream);
+/* Likelihood::evaluate (src/Likelihood.cpp:8-33) in one call:
+ *   *logL = sum_i sum_k counts_i[k] log max(1e-44, q_i[k]),  q_i = block sums of exp(times[i] A(c)) p0,
+ * the Krylov solve (m, tol as cufsp_expv_create) carrying p through the data times on the device and
+ * every time's term reduced there.  coefs: host, n_reactions (NULL: A's tcoef(0)); times: host,
+ * non-decreasing; d_p0: device, n states (not modified); d_counts: device, n_times x n / block;
+ * *fsp_error (nullable): sum p0 - sum p(times[last]), the FSP truncation error.  Synchronous. */
+cufsp_status cufsp_likelihood_eval(cufsp_mat *A, const double *coefs, int n_times, const double *times,
+                                   const double *d_p0, int64_t block, const double *d_counts, int m, double tol,
+                                   double *logL, double *fsp_error, cufsp_stream_t stream);
 /* Gradient of the log-likelihood above over several data times by the adjoint method (no counterpart
  * in the reference; its Likelihood has no gradient):
  *   log L(c) = sum_i sum_k counts_i[k] log max(1e-44, q_i[k]),  q_i = block sums of exp(times[i] A(c)) p0,

@@ -108,6 +108,8 @@ def ref() -> C.CDLL | None:
         R.ref_gpu_hyb_toggle.argtypes = [_P, _P, _P, _P]
         R.ref_gpu_kron.restype = _I
         R.ref_gpu_kron.argtypes = [_I, _I, _P, _P, _P, _P, _P, _P, _P, _P]
+        R.ref_gpu_hyb_tables.restype = _I
+        R.ref_gpu_hyb_tables.argtypes = [_I, _I, _P, _P, _P, _P, _P, _P, _P, _P, _I, _P]
         R.ref_gpu_kron_time.restype = _D
         R.ref_gpu_kron_time.argtypes = [_I, _I, _P, _P, _P, _P, _P, _P, _I]
         _ref = R

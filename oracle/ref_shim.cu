@@ -7,7 +7,8 @@
 //   host:  rect_fsp_num_states, indx2state, state2indx (src/cme_util.cu:5-22,55-62),
 //          fspmat_sdkron_fill_host_data (src/fspmat_kron_kernels.cu:170-190)
 //   GPU:   fsp_get_states (src/cme_util.cu:24-41), the HYB build + action
-//          (src/fspmat_hyb_kernels.cu:66-184) and the Kronecker action (src/fspmat_kron_kernels.cu:31-168).
+//          (src/fspmat_hyb_kernels.cu:66-184) with the toggle PropFun or a factor-table PropFun, and
+//          the Kronecker action (src/fspmat_kron_kernels.cu:31-168); both actions also timed.
 // The GPU entry points are only called with state counts that are multiples of 1024: the HYB action
 // has a __syncthreads() inside `if (tid < n_states)` (fspmat_hyb_kernels.cu:71-76) and the Kronecker
 // grid drops the last partial block (fspmat_kron_kernels.cu:42), so other sizes are not run.
@@ -36,6 +37,39 @@ __device__ double shim_toggle_propensity(int *x, int reaction) {
     }
 }
 __device__ cuFSP::PropFun shim_toggle_ptr = &shim_toggle_propensity;
+
+// A factor-table propensity a_r(x) = prod_s f_{r,s}(x_s) as a device PropFun, for running the
+// reference's HYB format on the product's factorised workloads (tables set by set_device_tables).
+__device__ const double *shim_dev_tables;
+__device__ int shim_dev_off[16];
+__device__ int shim_dev_stride;
+__device__ int shim_dev_ns;
+
+__device__ double shim_table_propensity(int *x, int reaction) {
+    const double *t = shim_dev_tables + (size_t)reaction * shim_dev_stride;
+    double v = 1.0;
+    for (int s = 0; s < shim_dev_ns; ++s) v *= t[shim_dev_off[s] + x[s]];
+    return v;
+}
+__device__ cuFSP::PropFun shim_table_ptr = &shim_table_propensity;
+
+// Copies the factor tables to the device for shim_table_propensity; returns the device copy.
+static double *set_device_tables(int ns, int nr, const int *bounds, const double *tables) {
+    int off[16] = {0};
+    int stride = 0;
+    for (int s = 0; s < ns && s < 16; ++s) {
+        off[s] = stride;
+        stride += bounds[s] + 1;
+    }
+    double *d_tab = nullptr;
+    cudaMalloc(&d_tab, sizeof(double) * (size_t)nr * stride);
+    cudaMemcpy(d_tab, tables, sizeof(double) * (size_t)nr * stride, cudaMemcpyHostToDevice);
+    cudaMemcpyToSymbol(shim_dev_tables, &d_tab, sizeof(d_tab));
+    cudaMemcpyToSymbol(shim_dev_off, off, sizeof(off));
+    cudaMemcpyToSymbol(shim_dev_stride, &stride, sizeof(int));
+    cudaMemcpyToSymbol(shim_dev_ns, &ns, sizeof(int));
+    return d_tab;
+}
 
 static const double *g_tables = nullptr;
 static std::vector<int> g_off;
@@ -142,6 +176,53 @@ int ref_gpu_kron(int ns, int nr, int *bounds, int *sv, int *sc, int *sr, const d
     cudaFree(d_x);
     cudaFree(d_y);
     kr.destroy();
+    return (int)e;
+}
+
+// The reference HYB format built through its own fill kernel with the factor-table PropFun above.
+// With x_host / y_host: y_host += sum_r coefs[r] A_r x_host (returns a CUDA error code).  With
+// iters > 0 and null vectors: `iters` actions on device buffers timed with cudaEvent, ms per action
+// returned through *ms.
+int ref_gpu_hyb_tables(int ns, int nr, int *bounds, int *sv, int *sc, int *sr, const double *tables,
+                       const double *coefs, const double *x_host, double *y_host, int iters, double *ms) {
+    int n = cuFSP::rect_fsp_num_states(ns, bounds);
+    if (n % 1024 != 0) return -1;
+    double *d_tab = set_device_tables(ns, nr, bounds, tables);
+    cuFSP::PropFun prop = nullptr;
+    cudaMemcpyFromSymbol(&prop, shim_table_ptr, sizeof(cuFSP::PropFun));
+    cuFSP::HYBMatSet hyb;
+    cuFSP::generate_fsp_mats_hyb(n, nr, ns, bounds, make_stoich(nr, ns, sv, sc, sr), prop, &hyb);
+    double *d_x = nullptr, *d_y = nullptr;
+    cudaMalloc(&d_x, (size_t)n * sizeof(double));
+    cudaMalloc(&d_y, (size_t)n * sizeof(double));
+    std::vector<double> c(coefs, coefs + nr);
+    cudaError_t e = cudaSuccess;
+    if (x_host && y_host) {
+        cudaMemcpy(d_x, x_host, (size_t)n * sizeof(double), cudaMemcpyHostToDevice);
+        cudaMemcpy(d_y, y_host, (size_t)n * sizeof(double), cudaMemcpyHostToDevice);
+        hyb.action(d_x, d_y, c.data());
+        e = cudaMemcpy(y_host, d_y, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost);
+    } else if (iters > 0 && ms) {
+        cudaMemset(d_x, 0, (size_t)n * sizeof(double));
+        cudaMemset(d_y, 0, (size_t)n * sizeof(double));
+        hyb.action(d_x, d_y, c.data());
+        cudaEvent_t a, b;
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+        cudaEventRecord(a);
+        for (int i = 0; i < iters; ++i) hyb.action(d_x, d_y, c.data());
+        cudaEventRecord(b);
+        e = cudaEventSynchronize(b);
+        float t = 0.f;
+        cudaEventElapsedTime(&t, a, b);
+        *ms = t / iters;
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+    }
+    cudaFree(d_x);
+    cudaFree(d_y);
+    cudaFree(d_tab);
+    hyb.destroy();
     return (int)e;
 }
 

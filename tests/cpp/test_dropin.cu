@@ -51,6 +51,7 @@ void t_func(double, double *out) {
 }
 
 static int failures = 0;
+static int cme_layer();
 #define EXPECT(cond, ...)                      \
     do {                                       \
         if (!(cond)) {                         \
@@ -143,6 +144,129 @@ int main() {
     }
     EXPECT(threw, "invalid bounds throw cuFSP::error");
 
+    failures += cme_layer();
     std::printf("%s (%d failures)\n", failures ? "FAILED" : "ok", failures);
     return failures ? 1 : 0;
+}
+
+// ---- the legacy cme:: layer (src/Model.h, src/FSPSolver.h, src/Likelihood.h) ------------------------
+// A gene-expression network: 3 binary genes, nuclear and cytoplasmic mRNA (12 reactions), box
+// (1,1,1,31,31).  The parameters are the 12 rates (t_fun unset).  The program prints the
+// log-likelihood and its gradient for the pytest wrapper, which recomputes both with the oracle.
+namespace {
+double gene_factor(int x, int species, int reaction) {
+    if (reaction < 3 && species == reaction) return 1.0 - x;
+    if (reaction >= 3 && reaction < 6 && species == reaction - 3) return 1.0 * x;
+    if (reaction >= 6 && reaction < 9 && species == reaction - 6) return 1.0 * x;
+    if ((reaction == 9 || reaction == 10) && species == 3) return 1.0 * x;
+    if (reaction == 11 && species == 4) return 1.0 * x;
+    return 1.0;
+}
+// the same propensities as a host function of a batch of states (the reference's Model::propensity)
+void gene_propensity(const int *states, int n_states, int n_species, double *props) {
+    for (int k = 0; k < n_states; ++k)
+        for (int r = 0; r < 12; ++r) {
+            double v = 1.0;
+            for (int s = 0; s < n_species; ++s) v *= gene_factor(states[k * n_species + s], s, r);
+            props[r * n_states + k] = v;
+        }
+}
+cme::Model gene_model(bool factorised) {
+    cme::Model m;
+    m.FSPSize = {1, 1, 1, 31, 31};
+    m.stoich_mat.assign(5, std::vector<int>(12, 0));
+    for (int i = 0; i < 3; ++i) {
+        m.stoich_mat[i][i] = 1;
+        m.stoich_mat[i][3 + i] = -1;
+        m.stoich_mat[3][6 + i] = 1;
+    }
+    m.stoich_mat[3][9] = -1;
+    m.stoich_mat[4][9] = 1;
+    m.stoich_mat[3][10] = -1;
+    m.stoich_mat[4][11] = -1;
+    m.states_init = {{0, 0, 0, 0, 0}};
+    m.probs_init = {1.0};
+    m.parameters = {0.05, 0.04, 0.03, 2.0, 2.0, 3.0, 0.5, 1.5, 2.0, 0.5, 0.1, 0.05};
+    if (factorised) m.prop_factor = &gene_factor;
+    else m.propensity = &gene_propensity;
+    return m;
+}
+}  // namespace
+
+static int cme_layer() {
+    int fails = 0;
+    const std::vector<double> times = {1.0, 3.0, 8.0};
+    cme::Model mf = gene_model(true), mh = gene_model(false);
+    // FSPSolver through the output times, the factorised and the host-propensity generators
+    std::vector<double> pf, ph;
+    cme::FSPSolver sf(pf, mf, times, 1e-6), sh(ph, mh, times, 1e-6);
+    if (pf.size() != 8192 || pf[0] != 1.0) {
+        std::printf("FAIL: FSPSolver initial vector\n");
+        ++fails;
+    }
+    for (size_t it = 0; it < times.size(); ++it) {
+        sf.next_time();
+        sh.next_time();
+        double d = 0.0, mass = 0.0;
+        for (size_t i = 0; i < pf.size(); ++i) {
+            d += std::fabs(pf[i] - ph[i]);
+            mass += pf[i];
+        }
+        if (!(d <= 1e-8) || std::fabs(sf.current_time() - times[it]) > 0 || !(mass <= 1.0 + 1e-12)) {
+            std::printf("FAIL: FSPSolver at t=%g: |p_kron - p_hyb|_1 = %g, mass %.17g\n", times[it], d, mass);
+            ++fails;
+        }
+        if (std::fabs(sf.fsp_error() - (1.0 - mass)) > 1e-12) {
+            std::printf("FAIL: fsp_error %g vs 1 - mass %g\n", sf.fsp_error(), 1.0 - mass);
+            ++fails;
+        }
+    }
+    const std::vector<double> p_end(pf);
+    // reset_time re-reads P: the caller returns it to the initial condition (Likelihood.cpp:24-30)
+    std::fill(pf.begin(), pf.end(), 0.0);
+    pf[0] = 1.0;
+    sf.reset_time();
+    sf.solve();
+    double dr = 0.0;
+    for (size_t i = 0; i < pf.size(); ++i) dr += std::fabs(pf[i] - p_end[i]);
+    if (!(dr <= 1e-12)) {
+        std::printf("FAIL: solve after reset_time differs by %g\n", dr);
+        ++fails;
+    }
+    // data, likelihood and gradient
+    cme::SingleCellData data = cme::generate_data(mf, times, {0, 0, 0, 0, 0}, 500, 777ULL);
+    if (data.snapshots.size() != times.size() || data.snapshots[0].size() != 500 * 5) {
+        std::printf("FAIL: generate_data shape\n");
+        ++fails;
+    }
+    cme::Likelihood L(data, mf);
+    L.set_krylov(30, 1e-10);
+    const double ll = L.evaluate(mf.parameters);
+    double ll_g = 0.0;
+    const std::vector<double> g = L.gradient(mf.parameters, &ll_g);
+    if (!(std::fabs(ll - ll_g) <= 1e-8 * std::fabs(ll))) {
+        std::printf("FAIL: evaluate %.17g vs gradient's log L %.17g\n", ll, ll_g);
+        ++fails;
+    }
+    cme::Likelihood Lh(data, mh);  // the host-propensity model evaluates too (no gradient)
+    Lh.set_krylov(30, 1e-10);
+    const double llh = Lh.evaluate(mh.parameters);
+    if (!(std::fabs(ll - llh) <= 1e-8 * std::fabs(ll))) {
+        std::printf("FAIL: log L kron %.17g vs hyb %.17g\n", ll, llh);
+        ++fails;
+    }
+    bool threw = false;
+    try {
+        Lh.gradient(mh.parameters);
+    } catch (const cuFSP::error &e) {
+        threw = e.status == CUFSP_ERR_UNSUPPORTED;
+    }
+    if (!threw) {
+        std::printf("FAIL: gradient of a host-propensity model must be refused\n");
+        ++fails;
+    }
+    std::printf("CME logL %.17g\nCME grad", ll);
+    for (double v : g) std::printf(" %.17g", v);
+    std::printf("\n");
+    return fails;
 }

@@ -208,6 +208,23 @@ def test_against_reference_gpu_kernels(cuda):
         A.action(0.0, dev(x), y)
         scale = oracle.assemble_model(m).abs_spmv(c, x).max()
         assert np.abs(host(y) - y_ref).max() <= 1e-13 * scale
+    # HYB built by the reference's own fill kernel from a factor-table PropFun, on the 3-species 32^3
+    # and the 5-species gene workloads
+    for m in (models.mass_action_3(31), models.gene_expression((1, 1, 1, 31, 31), time_varying=False)):
+        b = np.asarray(m.bounds, np.int32)
+        sv, sc, sr = m.stoich_csr()
+        tab = np.ascontiguousarray(m.tables)
+        c = np.ascontiguousarray(m.coefs(0))
+        x = rng.uniform(0, 1, m.n_states)
+        y_ref = np.zeros(m.n_states)
+        assert R.ref_gpu_hyb_tables(m.ns, m.nr, b.ctypes.data, sv.ctypes.data, sc.ctypes.data, sr.ctypes.data,
+                                    tab.ctypes.data, c.ctypes.data, x.ctypes.data, y_ref.ctypes.data, 0, None) == 0
+        scale = oracle.assemble_model(m).abs_spmv(c, x).max()
+        for fmt in (MatrixFormat.KRONECKER, MatrixFormat.HYB):
+            A = FSPMat.from_model(m, fmt)
+            y = dev(np.zeros(m.n_states))
+            A.action(0.0, dev(x), y)
+            assert np.abs(host(y) - y_ref).max() <= 1e-13 * scale, (m.name, fmt)
     # Kronecker on the 2-species (32,768 states) and 3-species 32^3 workloads
     for m in (models.birth_death_2(), models.mass_action_3(31)):
         b = np.asarray(m.bounds, np.int32)
