@@ -635,6 +635,92 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_leg(args):
+    """One leg alone, for profiling its kernels under ncu (small steps, one JSON line, no extras):
+      sparse  the CSR/HYB generator action y += A x on mass_action_3 (--box, default 255^3)
+      krylov  Krylov steps exp(tA)p0 on mass_action_3 (--box; above 2^20 states the launch sequence
+              of plane-kernel matvecs and the k_mdot / k_mupd / k_comb vector kernels)
+      adjoint one log-likelihood gradient on the gene model (--box, default 1,1,1,127,127)
+      bdf     the BDF solve of the time-varying gene model to t = 6 (--box)
+      states  state enumeration cufsp_get_states (--box, default 1023,1023,3)"""
+    import torch
+    from cuda_fsp_b200 import (BDFIntegrator, FSPMat, KryExpvFSP, Likelihood, MatrixFormat, get_states, models)
+    box = [int(v) for v in args.box.split(",")] if args.box else None
+    torch.cuda.set_device(0)
+    out = {"leg": args.leg, "profiling_run": True}
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if args.leg == "sparse":
+        m = models.mass_action_3(bounds=box) if box else models.mass_action_3()
+        A = FSPMat.from_model(m, MatrixFormat.HYB)
+        g = torch.Generator(device="cuda").manual_seed(5)
+        xs = [torch.rand(m.n_states, dtype=torch.float64, device="cuda", generator=g) for _ in range(2)]
+        ys = [torch.zeros(m.n_states, dtype=torch.float64, device="cuda") for _ in range(2)]
+        c = m.coefs(0)
+        for i in range(max(3, args.warmup)):
+            A.apply(xs[i % 2], ys[i % 2], coefs=c, beta=1.0)
+        torch.cuda.synchronize()
+        ev0.record()
+        for i in range(args.steps):
+            A.apply(xs[i % 2], ys[i % 2], coefs=c, beta=1.0)
+        ev1.record()
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1) / args.steps
+        bps = 24 + 8 * m.nr
+        out.update({"n_states": m.n_states, "us_per_action": round(ms * 1e3, 2), "bytes_per_state": bps,
+                    "gbs": round(bps * m.n_states / (ms * 1e-3) / 1e9, 1), "kernel": A.describe()})
+    elif args.leg == "krylov":
+        m = models.mass_action_3(bounds=box) if box else models.mass_action_3()
+        A = FSPMat.from_model(m, MatrixFormat.KRONECKER)
+        v = torch.as_tensor(m.p0(), device="cuda")
+        E = KryExpvFSP(20.0, A, v, m=args.krylov_m, tol=1e-8, coefs=m.coefs(0), iop=args.iop > 0, q_iop=max(1, args.iop))
+        for _ in range(max(1, args.warmup)):
+            E.step()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            E.step()
+        torch.cuda.synchronize()
+        dt = (time.perf_counter() - t0) / args.steps
+        out.update({"n_states": m.n_states, "ms_per_krylov_step": round(dt * 1e3, 3), "t_now": E.stats["t_now"],
+                    "m": args.krylov_m, "iop_q": args.iop})
+    elif args.leg == "adjoint":
+        m = models.gene_expression(tuple(box) if box else (1, 1, 1, 127, 127), time_varying=False)
+        times = np.geomspace(1.0, 60.0, 8)
+        rng = np.random.default_rng(1)
+        counts = rng.integers(0, 3, size=(8, m.n_states // 8)).astype(float)
+        L = Likelihood(m, times, counts, n_marginal=3, kry_tol=1e-8)
+        L.gradient()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            L.gradient()
+        torch.cuda.synchronize()
+        out.update({"n_states": m.n_states, "s_per_gradient": round((time.perf_counter() - t0) / args.steps, 4)})
+    elif args.leg == "bdf":
+        m = models.gene_expression(tuple(box) if box else (1, 1, 1, 127, 127), time_varying=True)
+        A = FSPMat.from_model(m, MatrixFormat.KRONECKER)
+        p = torch.as_tensor(m.p0(), device="cuda")
+        B = BDFIntegrator(A, rtol=1e-8, atol=1e-14)
+        t0 = time.perf_counter()
+        B.init(0.0, p)
+        B.advance(6.0, p)
+        torch.cuda.synchronize()
+        out.update({"n_states": m.n_states, "s_to_t6": round(time.perf_counter() - t0, 4), "steps": B.stats["n_steps"]})
+    elif args.leg == "states":
+        b = box or [1023, 1023, 3]
+        st = get_states(b)
+        torch.cuda.synchronize()
+        ev0.record()
+        for _ in range(args.steps):
+            st = get_states(b)
+        ev1.record()
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1) / args.steps
+        out.update({"n_states": int(st.shape[0]), "ms_per_call": round(ms, 4),
+                    "gbs_written": round(st.numel() * 4 / (ms * 1e-3) / 1e9, 1)})
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -644,7 +730,15 @@ def main():
     ap.add_argument("--sets", type=int, default=4, help="rotating (x, y) input pairs")
     ap.add_argument("--no-extras", action="store_true",
                     help="time the generator action only (no e2e, expmv or CPU legs); for profiling runs")
+    ap.add_argument("--leg", choices=["sparse", "krylov", "adjoint", "bdf", "states"], default=None,
+                    help="run one leg alone (profiling runs; see run_leg)")
+    ap.add_argument("--box", default=None, help="box bounds of the leg, comma separated")
+    ap.add_argument("--krylov-m", type=int, default=30, help="Krylov dimension of the krylov leg")
+    ap.add_argument("--iop", type=int, default=0, help="incomplete orthogonalisation depth q of the krylov leg (0: full)")
     args = ap.parse_args()
+    if args.leg:
+        run_leg(args)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

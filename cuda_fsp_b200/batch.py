@@ -176,16 +176,37 @@ def partition_instances(sizes, world: int) -> list[list[int]]:
     return [sorted(p) for p in parts]
 
 
+def _gather_flat(local: np.ndarray, counts: list[int], group=None) -> list[np.ndarray]:
+    """all_gather of variable-length float64 vectors whose lengths every rank knows (`counts[r]`):
+    padded to the longest, gathered as tensors (NCCL: device tensors, gloo: host tensors), trimmed."""
+    import torch
+    import torch.distributed as dist
+    world = len(counts)
+    width = max(1, max(counts))
+    dev = torch.device("cuda", torch.cuda.current_device()) if dist.get_backend(group) == "nccl" else torch.device("cpu")
+    buf = torch.zeros(width, dtype=torch.float64, device=dev)
+    if local.size:
+        buf[: local.size] = torch.from_numpy(np.ascontiguousarray(local, np.float64)).to(dev)
+    parts = [torch.empty(width, dtype=torch.float64, device=dev) for _ in range(world)]
+    dist.all_gather(parts, buf, group=group)
+    return [parts[r][: counts[r]].cpu().numpy() for r in range(world)]
+
+
 def solve_sharded(models_, t_final: float, rank: int, world: int, m: int = 30, tol: float = 1e-8,
-                  solver=None, group=None) -> list[dict]:
+                  solver=None, group=None, gather: str = "summary", reduce=None) -> list:
     """Solve this rank's share of the instances (exp(t_final A_i) p_i(0) from each model's p0) and
-    gather every instance's summary (final mass, steps, status) on all ranks -- the only collective.
+    gather the results on all ranks -- the only collective.  `gather`:
+      "summary"  every instance's final mass, steps and status (a dict per instance);
+      "vectors"  the solution vectors themselves (a float64 array per instance, one padded tensor
+                 all_gather of each rank's packed vectors);
+      "reduce"   reduce(model, vector, stat) computed on the owning rank, gathered as objects (for
+                 caller-chosen reductions: marginals, moments, likelihood terms).
     `solver(models, t)` -> list of (vector, stat) may replace the GPU batch (host tests)."""
     import torch.distributed as dist
 
     parts = partition_instances([mm.n_states for mm in models_], world)
     mine = parts[rank]
-    local: list[tuple[int, dict]] = []
+    vecs, stats = [], []
     if mine:
         sub = [models_[i] for i in mine]
         if solver is None:
@@ -195,15 +216,54 @@ def solve_sharded(models_, t_final: float, rank: int, world: int, m: int = 30, t
             vecs = B.unpack(p)
         else:
             vecs, stats = zip(*solver(sub, t_final))
-        for i, v, st in zip(mine, vecs, stats):
-            local.append((i, {"mass": float(np.sum(v)), "steps": int(st["steps"]), "status": int(st["status"])}))
+    if gather == "vectors":
+        local = np.concatenate([np.asarray(v, np.float64) for v in vecs]) if mine else np.zeros(0)
+        counts = [int(sum(models_[i].n_states for i in part)) for part in parts]
+        flat = [local] if world == 1 else _gather_flat(local, counts, group)
+        out: list = [None] * len(models_)
+        for r, part in enumerate(parts):
+            off = 0
+            for i in part:
+                n = models_[i].n_states
+                out[i] = flat[r][off:off + n]
+                off += n
+        return out
+    if gather == "reduce":
+        if reduce is None:
+            raise ValueError("gather='reduce' needs reduce(model, vector, stat)")
+        local = [(i, reduce(models_[i], v, st)) for i, v, st in zip(mine, vecs, stats)]
+    elif gather == "summary":
+        local = [(i, {"mass": float(np.sum(v)), "steps": int(st["steps"]), "status": int(st["status"])})
+                 for i, v, st in zip(mine, vecs, stats)]
+    else:
+        raise ValueError(f"unknown gather mode {gather!r}")
     if world == 1:
         gathered = [local]
     else:
         gathered = [None] * world
         dist.all_gather_object(gathered, local, group=group)
-    out: list[dict] = [{} for _ in models_]
+    out = [None] * len(models_)
     for part in gathered:
-        for i, summary in part:
-            out[i] = summary
+        for i, value in part:
+            out[i] = value
     return out
+
+
+def gradient_sharded(likelihood, coef_sets, rank: int, world: int, workers: int = 2, group=None, grad_fn=None):
+    """d log L / d log c for many parameter sets over several GPUs: the sets are split into `world`
+    contiguous blocks, each rank computes its block (Likelihood.gradient_batched, or grad_fn(sets) ->
+    (logL [k], grad [k, nr]) in host tests), and one all_gather of the packed (log L, gradient) rows
+    gives every rank all of them.  Returns (logL [n_sets], grad [n_sets, n_reactions])."""
+    c = np.asarray(coef_sets, np.float64)
+    n_sets, nr = c.shape
+    bounds = [n_sets * r // world for r in range(world + 1)]
+    lo, hi = bounds[rank], bounds[rank + 1]
+    if hi > lo:
+        ll, g = (grad_fn or (lambda s: likelihood.gradient_batched(s, workers=workers)))(c[lo:hi])
+        local = np.concatenate([np.asarray(ll, np.float64)[:, None], np.asarray(g, np.float64)], axis=1).ravel()
+    else:
+        local = np.zeros(0)
+    counts = [(bounds[r + 1] - bounds[r]) * (nr + 1) for r in range(world)]
+    flat = [local] if world == 1 else _gather_flat(local, counts, group)
+    rows = np.concatenate([f.reshape(-1, nr + 1) for f in flat], axis=0)
+    return rows[:, 0].copy(), rows[:, 1:].copy()

@@ -367,7 +367,9 @@ __device__ __forceinline__ void plane_mv(const CufspPlaneArgs &a, const double *
     const bool prologue_ok = !bad;
 
     int z = t.z0;
-    // Refill after a CTA barrier: the stages released by the step go to the next planes.
+    // Refill after a CTA barrier: every stage whose plane the CTA has finished with goes to the next
+    // plane at once -- after the prologue the halo plane z0 - 1, after step z plane z (its x rows went
+    // into the register queue one step earlier, its y rows and words were used in step z).
     auto refill = [&](int count) {
         if (tid == 0)
             for (int k = 0; k < count && issued < p_last; ++k) {
@@ -376,6 +378,7 @@ __device__ __forceinline__ void plane_mv(const CufspPlaneArgs &a, const double *
                 issue_plane<ACCUM>(a, t, x, y, stage_of(issued), bars + (issued - pbase) % S, issued);
             }
     };
+    if (!bad) refill(1);
     if constexpr (PPS == 1) {
         // Step z: the slots hold (z - 1, z, z + 1) in a fixed rotation of 3; one barrier per plane.
         auto step = [&](Slot &sm, Slot &s0, Slot &sp) -> bool {
