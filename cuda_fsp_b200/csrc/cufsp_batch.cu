@@ -291,7 +291,8 @@ std::string tune_key(const cufsp_batch *B) {
 }
 
 // Autotuner: time each candidate launch shape on a sample of the batch (copies of the caller's
-// vectors) and keep the fastest.
+// vectors) over a sixteenth of the requested horizon (a few Krylov steps per instance: the cost per
+// step, not the horizon, separates the shapes) and keep the fastest.
 cufsp_status autotune(cufsp_batch *B, double t_final, const double *p, cudaStream_t st) {
     const std::string key = tune_key(B);
     Shape sh{env_int("CUFSP_BATCH_CLUSTER", 0), env_int("CUFSP_BATCH_THREADS", 0), env_int("CUFSP_BATCH_MINB", 1)};
@@ -321,8 +322,8 @@ cufsp_status autotune(cufsp_batch *B, double t_final, const double *p, cudaStrea
             if (ensure_work(B, ncl) != CUFSP_SUCCESS) continue;
             CUFSP_CUDA_TRY(cudaMemcpyAsync(B->d_scratch, p, sizeof(double) * (size_t)total, cudaMemcpyDeviceToDevice, st));
             CUFSP_CUDA_TRY(cudaEventRecord(e0, st));
-            cufsp_status s =
-                launch(B, *k, cd.cluster, cd.threads, ncl, t_final, B->d_scratch, B->d_order_sample, B->n_sample, st);
+            cufsp_status s = launch(B, *k, cd.cluster, cd.threads, ncl, t_final / 16.0, B->d_scratch, B->d_order_sample,
+                                    B->n_sample, st);
             CUFSP_CUDA_TRY(cudaEventRecord(e1, st));
             if (s != CUFSP_SUCCESS || cudaStreamSynchronize(st) != cudaSuccess) {
                 cudaGetLastError();
@@ -448,10 +449,13 @@ extern "C" cufsp_status cufsp_batch_create(const cufsp_batch_desc *d, int m, dou
     B->order.resize(ni);
     std::iota(B->order.begin(), B->order.end(), 0);
     std::stable_sort(B->order.begin(), B->order.end(), [&](int a, int b) { return B->inst[a].n > B->inst[b].n; });
-    // autotuner sample: every k-th instance of the size-sorted order, at most 32
+    // autotuner sample: every k-th instance of the size-sorted order, up to 96 -- more instances than
+    // any candidate shape has clusters (148 SMs in clusters of 4 CTAs at 2 CTAs per SM: 74), so that
+    // every candidate is timed with all of its clusters busy, as in the full batch
+    constexpr int kSampleMax = 96;
     std::vector<int> sample;
-    const int stride_s = std::max(1, ni / 32);
-    for (int i = 0; i < ni && (int)sample.size() < 32; i += stride_s) sample.push_back(B->order[i]);
+    const int stride_s = std::max(1, ni / kSampleMax);
+    for (int i = 0; i < ni && (int)sample.size() < kSampleMax; i += stride_s) sample.push_back(B->order[i]);
     B->n_sample = (int)sample.size();
 
     std::ostringstream s;
