@@ -11,7 +11,7 @@ the full state vector through the C ABI (cufsp_mat_apply, accumulate form).
             D2H of y inside the timed region
   roofline  the kernel's achieved GB/s against the measured HBM copy bandwidth
   cpu_baseline  the FP64 host oracle (OpenMP CSR SpMV restating the reference's assembly) timed on
-            the host cores on a bounded sample (box 255 x 255 x 63, about 10 s)
+            the host cores on the same 255^3 workload (about 10 s of steps)
   secondary [expmv solves/s on birth_death_2 (32,768 states, t = 10, m = 30, tol 1e-8) with the
              oracle's host solve time beside it;
              batched expmv solves/s on 256 gene-expression parameter sets (one persistent launch) with
@@ -44,7 +44,14 @@ METRIC = "matvec HBM GB/s; expmv solves/s & ∇logL grads/s at 1e-8 err vs plain
 BYTES_PER_STATE = 24
 WORKLOAD = ("mass_action_3 generator action y += A(t)x: 3 species, 9 reactions, box 255^3 = 16,777,216 states, "
             "KRONECKER matrix-free, FP64")
-CPU_SAMPLE_BOUNDS = (255, 255, 63)
+CPU_BOUNDS = (255, 255, 255)  # the CPU baseline runs the same workload as the GPU arm
+
+
+def workload_config(world: int) -> dict:
+    """The `config` of both arms' lines (identical, so that the two lines describe one workload)."""
+    return {"workload": WORKLOAD, "n_states": 16777216, "format": "KRONECKER", "form": "y += A x",
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+            "l2": "4 rotating (x, y) input pairs, 1.07 GB > 126 MB L2", "bytes_per_state": BYTES_PER_STATE}
 
 
 def measured_peak_hbm() -> tuple[float, str]:
@@ -159,9 +166,10 @@ def dist_setup():
     return world, rank, local
 
 
-def cpu_oracle_gbs(min_steps: int, warmup: int, bounds=CPU_SAMPLE_BOUNDS, budget_s: float = 10.0) -> dict:
-    """Time the oracle's OpenMP CSR SpMV (y += A x) on a bounded sample of the workload: at least
-    `min_steps` steps and about `budget_s` seconds of CPU work."""
+def cpu_oracle_gbs(min_steps: int, warmup: int = 3, bounds=CPU_BOUNDS, budget_s: float = 10.0) -> dict:
+    """Time the oracle's OpenMP CSR SpMV (y += A x, restating the reference's per-reaction CSR
+    assembly) on the workload itself: `warmup` untimed steps, then at least `min_steps` steps and
+    about `budget_s` seconds of CPU work, all host threads."""
     import oracle
     from cuda_fsp_b200 import models
     m = models.mass_action_3(bounds=bounds)
@@ -180,7 +188,8 @@ def cpu_oracle_gbs(min_steps: int, warmup: int, bounds=CPU_SAMPLE_BOUNDS, budget
     dt = (time.perf_counter() - t0) / steps
     return {"value": BYTES_PER_STATE * m.n_states / dt / 1e9, "unit": "GB/s", "cores": oracle.num_threads(),
             "kind": "port", "sample": f"oracle CSR SpMV y += A x on box {bounds[0]}x{bounds[1]}x{bounds[2]} "
-                                      f"({m.n_states} states, same 9-reaction model), {steps} steps",
+                                      f"({m.n_states} states, the 9-reaction workload), {steps} steps after "
+                                      f"{max(1, warmup)} untimed",
             "ms_per_step": dt * 1e3}
 
 
@@ -232,11 +241,11 @@ def run_reference(args):
     if rank != 0:
         return
     steps = max(1, args.steps)
-    cb = cpu_oracle_gbs(steps, max(1, min(args.warmup, 2)))
+    cb = cpu_oracle_gbs(steps, max(3, args.warmup))
     line = {"impl": "reference", "metric": METRIC, "value": round(cb["value"], 3), "unit": "GB/s",
             "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup, "ms_per_step": round(cb["ms_per_step"], 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": {"workload": WORKLOAD, "sample": cb["sample"]},
+            "data": "synthetic", "config": workload_config(args.gpus),
             "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
             "e2e": {"value": round(cb["value"], 3), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     gk = reference_gpu_kernel()
@@ -605,17 +614,14 @@ def run_ours(args):
         secondary["cpu_oracle_ms_per_solve"] = round(cpu_expmv_ms(), 1)
         secondary = [secondary, sparse_secondary(), bdf_secondary(), expmv_large_secondary(), batched_secondary(),
                      gradient_secondary()]
-    cpu = cpu_oracle_gbs(max(3, min(args.steps, 20)), 1) if (rank == 0 and world == 1) else None
+    cpu = cpu_oracle_gbs(max(3, min(args.steps, 20)), 3) if (rank == 0 and world == 1) else None
     peak, peak_kind = measured_peak_hbm()
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms, 5), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "n_states": n, "format": "KRONECKER", "form": "y += A x",
-                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                       "l2": "4 rotating (x, y) input pairs, 1.07 GB > 126 MB L2",
-                       "bytes_per_state": BYTES_PER_STATE},
+            "config": workload_config(world),
             "e2e": {"value": round(e2e_gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": 16 * n, "d2h_bytes_per_step": 8 * n,
                     "entry_point": "cufsp_mat_action_host", "ms_per_step": round(e2e_s * 1e3, 3)},
             "roofline": {"bound": "hbm", "achieved": round(kernel_gbs, 3), "peak": peak, "unit": "GB/s",
@@ -641,6 +647,7 @@ def run_leg(args):
       krylov  Krylov steps exp(tA)p0 on mass_action_3 (--box; above 2^20 states the launch sequence
               of plane-kernel matvecs and the k_mdot / k_mupd / k_comb vector kernels)
       adjoint one log-likelihood gradient on the gene model (--box, default 1,1,1,127,127)
+      gradbatch  gradients of --sets parameter sets with --workers concurrent host workers
       bdf     the BDF solve of the time-varying gene model to t = 6 (--box)
       states  state enumeration cufsp_get_states (--box, default 1023,1023,3)"""
     import torch
@@ -696,6 +703,21 @@ def run_leg(args):
             L.gradient()
         torch.cuda.synchronize()
         out.update({"n_states": m.n_states, "s_per_gradient": round((time.perf_counter() - t0) / args.steps, 4)})
+    elif args.leg == "gradbatch":
+        m = models.gene_expression(tuple(box) if box else (1, 1, 1, 127, 127), time_varying=False)
+        times = np.geomspace(1.0, 60.0, 8)
+        rng = np.random.default_rng(1)
+        counts = rng.integers(0, 3, size=(8, m.n_states // 8)).astype(float)
+        L = Likelihood(m, times, counts, n_marginal=3, kry_tol=1e-8)
+        sets = np.stack([m.coefs(0) * 10.0 ** rng.uniform(-0.5, 0.5, m.nr) for _ in range(args.sets)])
+        L.gradient(sets[0])
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        L.gradient_batched(sets, workers=args.workers)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        out.update({"n_states": m.n_states, "sets": args.sets, "workers": args.workers,
+                    "grads_per_s": round(args.sets / dt, 3)})
     elif args.leg == "bdf":
         m = models.gene_expression(tuple(box) if box else (1, 1, 1, 127, 127), time_varying=True)
         A = FSPMat.from_model(m, MatrixFormat.KRONECKER)
@@ -727,12 +749,13 @@ def main():
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--sets", type=int, default=4, help="rotating (x, y) input pairs")
+    ap.add_argument("--sets", type=int, default=4, help="rotating (x, y) input pairs; parameter sets of the gradbatch leg")
     ap.add_argument("--no-extras", action="store_true",
                     help="time the generator action only (no e2e, expmv or CPU legs); for profiling runs")
-    ap.add_argument("--leg", choices=["sparse", "krylov", "adjoint", "bdf", "states"], default=None,
+    ap.add_argument("--leg", choices=["sparse", "krylov", "adjoint", "gradbatch", "bdf", "states"], default=None,
                     help="run one leg alone (profiling runs; see run_leg)")
     ap.add_argument("--box", default=None, help="box bounds of the leg, comma separated")
+    ap.add_argument("--workers", type=int, default=2, help="host workers of the gradbatch leg")
     ap.add_argument("--krylov-m", type=int, default=30, help="Krylov dimension of the krylov leg")
     ap.add_argument("--iop", type=int, default=0, help="incomplete orthogonalisation depth q of the krylov leg (0: full)")
     args = ap.parse_args()

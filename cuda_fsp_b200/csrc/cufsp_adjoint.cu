@@ -463,13 +463,18 @@ extern "C" cufsp_status cufsp_likelihood_grad_batched(const cufsp_model_desc *de
         return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_likelihood_grad_batched: bad argument");
     const int nr = desc->n_reactions;
     workers = std::max(1, std::min(std::min(workers, n_sets), 32));
-    // Generators small enough for the persistent Arnoldi pass: one such pass fills the GPU, so two
-    // workers suffice (one solve's pass overlaps the other's host-side step control); larger
-    // generators run `workers` concurrent launch sequences.
+    // Generators small enough for the persistent Arnoldi pass: every worker's passes take an equal
+    // share of the SMs (CUFSP_GRAD_SM_SHARE=0: each pass takes all SMs and the passes of the workers
+    // take turns), so that the workers' solves run side by side; larger generators run `workers`
+    // concurrent launch sequences.
     int64_t n_states = 1;
     for (int s = 0; s < desc->n_species; ++s) n_states *= (int64_t)desc->fsp_bounds[s] + 1;
     const bool persistent = parnoldi_size_ok(n_states);
-    if (persistent) workers = std::min(workers, 2);
+    const char *share_env = getenv("CUFSP_GRAD_SM_SHARE");
+    const bool share = !share_env || atoi(share_env) != 0;
+    int cta_cap = 0;
+    if (persistent && share) cta_cap = std::max(1, device_info().sm_count / workers);
+    else if (persistent) workers = std::min(workers, 2);
     int dev = 0;
     CUFSP_CUDA_TRY(cudaGetDevice(&dev));
     std::atomic<int> next(0);
@@ -478,6 +483,7 @@ extern "C" cufsp_status cufsp_likelihood_grad_batched(const cufsp_model_desc *de
     auto work = [&](int w) {
         cudaSetDevice(dev);
         parnoldi_thread_disable(!persistent && workers > 1);
+        parnoldi_thread_cta_cap(cta_cap);
         cufsp_mat *A = nullptr;
         cudaStream_t st = nullptr;
         cufsp_status s = cufsp_mat_create(desc, CUFSP_FORMAT_KRONECKER, &A);
@@ -497,6 +503,7 @@ extern "C" cufsp_status cufsp_likelihood_grad_batched(const cufsp_model_desc *de
         if (st) cudaStreamDestroy(st);
         cufsp_mat_destroy(A);
         parnoldi_thread_disable(false);
+        parnoldi_thread_cta_cap(0);
     };
     std::vector<std::thread> pool;
     for (int w = 1; w < workers; ++w) pool.emplace_back(work, w);

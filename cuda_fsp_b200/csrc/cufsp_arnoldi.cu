@@ -379,6 +379,11 @@ void parnoldi_destroy(PArnoldi *pa, cudaStream_t last_use) {
 void parnoldi_thread_disable(bool off) { tl_disabled = off; }
 
 namespace {
+thread_local int tl_cta_cap = 0;  // at most this many CTAs per pass launched from this thread (0: all SMs)
+}
+void parnoldi_thread_cta_cap(int cap) { tl_cta_cap = cap > 0 ? cap : 0; }
+
+namespace {
 int persistent_mode() {  // CUFSP_ARNOLDI_PERSISTENT: 0 never, 1 always, unset: by size
     static const int mode = [] {
         const char *e = getenv("CUFSP_ARNOLDI_PERSISTENT");
@@ -533,7 +538,9 @@ cufsp_status parnoldi_run(PArnoldi **ppa, cufsp_mat *A, const std::vector<double
             const char *e = getenv("CUFSP_ARNOLDI_CTA_STATES");
             return e ? std::max<int64_t>(32, atoll(e)) : (int64_t)256;
         }();
-        const int sms = device_info().sm_count;
+        // a host thread that shares the GPU with other solves (the batched gradient's workers) takes
+        // its share of the SMs, so that the workers' cooperative passes run side by side
+        const int sms = tl_cta_cap > 0 ? std::min(tl_cta_cap, device_info().sm_count) : device_info().sm_count;
         const int64_t want = std::max<int64_t>(1, std::min<int64_t>(sms, (n + min_states - 1) / min_states));
         const int64_t chunk = (n + want - 1) / want;
         const int64_t grid = (n + chunk - 1) / chunk;

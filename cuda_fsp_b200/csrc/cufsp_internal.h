@@ -237,6 +237,9 @@ void parnoldi_destroy(PArnoldi *pa, cudaStream_t last_use);  // every launch of 
 // Host threads that run many solves concurrently keep the launch sequence: the persistent pass
 // wants every SM to itself.
 void parnoldi_thread_disable(bool off);
+// Passes launched later from this host thread use at most `cap` CTAs (one per SM; 0: every SM), so
+// that several threads' passes share the GPU side by side.
+void parnoldi_thread_cta_cap(int cap);
 
 // Internals of the single-instance Krylov driver used by the adjoint gradient (cufsp_krylov.cu).
 void expv_set_transpose(cufsp_expv *E, bool transpose);
