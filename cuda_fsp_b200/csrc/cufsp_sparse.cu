@@ -171,12 +171,14 @@ void sparse_build_rtc(const ModelHost &m, SparseData *sd, std::string &why) {
         stride[s] = st;
         st *= (int64_t)m.bounds[s] + 1;
     }
-    // reactions whose loads are in flight together, and CTAs per SM the launch bounds promise
-    // (CUFSP_SPARSE_CHUNK / CUFSP_SPARSE_MINB override them for tuning)
+    // Reactions whose loads are in flight together, and CTAs per SM the launch bounds promise
+    // (CUFSP_SPARSE_CHUNK / CUFSP_SPARSE_MINB override them for tuning).  Measured on the 255^3
+    // 9-reaction workload (B200): chunks of 5 at 2 CTAs per SM 275 us per action (5.86 TB/s), all 9
+    // at once 331 us, the generic kernel 748 us.
     const char *ec = getenv("CUFSP_SPARSE_CHUNK");
     const char *em = getenv("CUFSP_SPARSE_MINB");
-    const int chunk = std::max(1, std::min(m.nr, ec ? atoi(ec) : (m.nr <= 12 ? m.nr : 8)));
-    const int minb = std::max(1, std::min(8, em ? atoi(em) : 1));
+    const int chunk = std::max(1, std::min(m.nr, ec ? atoi(ec) : 5));
+    const int minb = std::max(1, std::min(8, em ? atoi(em) : 2));
     std::ostringstream o;
     o << "#define CUFSP_SPARSE_MINB " << minb << "\n";
     o << "#define CUFSP_SPARSE_RTC_MAX_R " << CUFSP_SPARSE_RTC_MAX_R << "\n#define CUFSP_SPARSE_NS " << m.ns

@@ -229,7 +229,9 @@ static int cme_layer() {
     sf.solve();
     double dr = 0.0;
     for (size_t i = 0; i < pf.size(); ++i) dr += std::fabs(pf[i] - p_end[i]);
-    if (!(dr <= 1e-12)) {
+    // solve() steps straight to the last time, so its Krylov steps differ from next_time()'s: the two
+    // agree within the Krylov tolerance
+    if (!(dr <= 1e-8)) {
         std::printf("FAIL: solve after reset_time differs by %g\n", dr);
         ++fails;
     }
