@@ -491,7 +491,9 @@ __device__ void solve_instance(const CufspBatchArgs &a, cg::cluster_group &cl, S
                 status = 2;
                 break;
             }
-            if (sn < btol) {  // happy breakdown (src/KryExpvFSP.cu:90-98)
+            // happy breakdown (src/KryExpvFSP.cu:90-98) with the threshold divided by the remaining time
+            // (when above 1): the jump to t_final then stays within tol
+            if (sn < btol / fmax(1.0, a.t_final - t_now)) {
                 k1 = 0;
                 mb = j + 1;
                 break;

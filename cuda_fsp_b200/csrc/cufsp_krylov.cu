@@ -33,7 +33,8 @@ constexpr int kMaxVec = CUFSP_MAX_KRYLOV + 1;
 //   H[(m+2)^2] | rho[m+2] | gam[m+2] | beta | avnorm | pad | pad | flag(int)
 struct KState {
     double *H, *rho, *gam, *beta, *avnorm;
-    int *flag;  // 0 ok, >0 happy breakdown at mb = flag, -1 NaN/Inf, -2 zero vector
+    double *btol;  // happy-breakdown threshold of the current pass (written by the host before the pass)
+    int *flag;     // 0 ok, >0 happy breakdown at mb = flag, -1 NaN/Inf, -2 zero vector
     int mp2;
 };
 
@@ -70,7 +71,6 @@ struct MVecArgs {
     int K;      // number of basis vectors used (istart..j)
     int kbase;  // istart
     int j;
-    double btol;
     KState s;
     double *partials;
     unsigned int *counter;
@@ -125,7 +125,7 @@ __global__ void __launch_bounds__(kRedThreads) k_mupd(const MVecArgs a) {
         const double sn = sqrt(sm.final_[0]);
         if (!isfinite(sn)) {
             *a.s.flag = -1;
-        } else if (sn < a.btol) {
+        } else if (sn < *a.s.btol) {
             *a.s.flag = a.j + 1;
         } else {
             a.s.H[(a.j + 1) + a.j * a.s.mp2] = sn;
@@ -186,6 +186,7 @@ struct cufsp_expv_s {
     double anorm = 1.0;
     int64_t max_nstep = 10000, max_reject = 1000;
     double t_final = 0.0, t_now = 0.0, t_new = 0.0, btol = 0.0, xm = 0.0;
+    double *h_btol = nullptr;  // pinned host copy of the pass's breakdown threshold (copied to ks.btol)
     int64_t i_step = 0;
     cufsp_mat *A = nullptr;
     std::vector<double> coefs;
@@ -245,7 +246,6 @@ cufsp_status arnoldi_dot_update(cufsp_expv *E, double *v, int j, int istart, cud
     a.w = wvec(E, v, j + 1);
     a.n = E->n;
     a.j = j;
-    a.btol = E->btol;
     a.s = E->ks;
     a.partials = E->rs.partials;
     a.counter = E->rs.counter;
@@ -302,7 +302,8 @@ bool graphs_enabled() {
 // flag; one device->host copy of the state block into E->hstate.  With a generator bound, the ~3m
 // launches are captured once per (vector, form) into a CUDA graph and replayed (one launch per
 // step); the generator's coefficient-dependent tables are prepared eagerly before each replay.
-cufsp_status arnoldi_pass(cufsp_expv *E, double *v, cudaStream_t st, bool with_avnorm) {
+// btol_eff: happy-breakdown threshold of this pass.
+cufsp_status arnoldi_pass(cufsp_expv *E, double *v, cudaStream_t st, bool with_avnorm, double btol_eff) {
     cufsp_status s;
     if (E->used && E->last_stream != st) E->mixed = true;
     E->used = true;
@@ -310,10 +311,12 @@ cufsp_status arnoldi_pass(cufsp_expv *E, double *v, cudaStream_t st, bool with_a
     const bool persistent = E->A && parnoldi_wanted(E->A, E->n, E->m);
     if (persistent) {
         s = parnoldi_run(&E->pa, E->A, E->coefs, E->transpose, E->n, v, E->W, E->ks.H, E->ks.rho, E->ks.gam,
-                         E->ks.beta, E->ks.avnorm, E->ks.flag, E->ks.flag + 1, E->m, E->iop, E->q_iop, E->btol,
+                         E->ks.beta, E->ks.avnorm, E->ks.flag, E->ks.flag + 1, E->m, E->iop, E->q_iop, btol_eff,
                          with_avnorm, st);
         if (s != CUFSP_SUCCESS) return s;
     } else if (E->A && graphs_enabled()) {
+        *E->h_btol = btol_eff;  // the previous pass's copy has completed: the stream was synchronised after it
+        CUFSP_CUDA_TRY(cudaMemcpyAsync(E->ks.btol, E->h_btol, sizeof(double), cudaMemcpyHostToDevice, st));
         s = mat_prepare(E->A, E->coefs.data(), st);
         if (s != CUFSP_SUCCESS) return s;
         cudaGraphExec_t exec = nullptr;
@@ -341,6 +344,8 @@ cufsp_status arnoldi_pass(cufsp_expv *E, double *v, cudaStream_t st, bool with_a
         }
         CUFSP_CUDA_TRY(cudaGraphLaunch(exec, st));
     } else {
+        *E->h_btol = btol_eff;
+        CUFSP_CUDA_TRY(cudaMemcpyAsync(E->ks.btol, E->h_btol, sizeof(double), cudaMemcpyHostToDevice, st));
         s = arnoldi_launches(E, v, st, with_avnorm);
         if (s != CUFSP_SUCCESS) return s;
     }
@@ -384,7 +389,12 @@ cufsp_status expv_step(cufsp_expv *E, double *v, cudaStream_t st) {
     const double delta = 1.2, gamma = 0.9;
     if (E->i_step == 0) E->btol = E->anorm * E->tol;  // tolerance for happy breakdown (:50)
 
-    cufsp_status s = arnoldi_pass(E, v, st, true);
+    // A happy breakdown ends the solve in one jump to t_final (:90-98) whose error grows like the
+    // residual times the remaining time; the reference accepts residuals below anorm * tol, i.e. an
+    // error of up to tol per unit of the remaining time.  Dividing the threshold by the remaining
+    // time (when above 1) keeps the jump's error within tol.
+    const double btol_eff = E->btol / std::max(1.0, E->t_final - E->t_now);
+    cufsp_status s = arnoldi_pass(E, v, st, true, btol_eff);
     if (s != CUFSP_SUCCESS) return s;
     const double *hH = E->hstate.data();
     const double *hrho = hH + (size_t)mp2 * mp2;
@@ -488,7 +498,9 @@ cufsp_status expv_step(cufsp_expv *E, double *v, cudaStream_t st) {
 
 namespace cufsp {
 void expv_set_transpose(cufsp_expv *E, bool transpose) { E->transpose = transpose; }
-cufsp_status expv_arnoldi(cufsp_expv *E, double *v, cudaStream_t st) { return arnoldi_pass(E, v, st, false); }
+cufsp_status expv_arnoldi(cufsp_expv *E, double *v, cudaStream_t st) {
+    return arnoldi_pass(E, v, st, false, E->btol > 0.0 ? E->btol : E->anorm * E->tol);
+}
 cufsp_status expv_step_once(cufsp_expv *E, double *v, cudaStream_t st) { return expv_step(E, v, st); }
 const KrylovStep &expv_last(const cufsp_expv *E) { return E->last; }
 const double *expv_basis(const cufsp_expv *E, const double *v, int k) {
@@ -533,7 +545,13 @@ extern "C" cufsp_status cufsp_expv_create(int64_t n, int m, double tol, int iop,
     E->ks.gam = E->ks.rho + mp2;
     E->ks.beta = E->ks.gam + mp2;
     E->ks.avnorm = E->ks.beta + 1;
+    E->ks.btol = E->ks.beta + 2;
     E->ks.flag = reinterpret_cast<int *>(E->ks.beta + 4);
+    if (cudaHostAlloc((void **)&E->h_btol, sizeof(double), cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        cufsp_expv_destroy(E);
+        return set_error(CUFSP_ERR_ALLOC, "cufsp_expv_create: pinned allocation failed");
+    }
     E->ks.mp2 = mp2;
     E->grid = stream_grid(n, 4, device_info().sm_count * 4);
     cufsp_status s = E->rs.init(E->grid, 64);
@@ -560,6 +578,7 @@ extern "C" cufsp_status cufsp_expv_destroy(cufsp_expv *E) {
         E->rs.release();
     }
     if (E->cap_stream) cudaStreamDestroy(E->cap_stream);
+    if (E->h_btol) cudaFreeHost(E->h_btol);
     delete E;
     return CUFSP_SUCCESS;
 }

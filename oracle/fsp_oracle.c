@@ -456,7 +456,10 @@ int orc_expv(int64_t n, int nr, const int *rowptr, const int *col, const double 
                 w[i] = acc;
             }
             double s = orc_nrm2(n, w);
-            if (s < btol) {
+            /* The reference's happy-breakdown test (KryExpvFSP.cu:90-98) with the threshold divided by
+             * the remaining time when above 1: the jump to t_final that follows then stays within tol
+             * (the reference's threshold allows an error of tol per unit of remaining time). */
+            if (s < btol / fmax(1.0, t_final - t_now)) {
                 k1 = 0;
                 mb = j + 1;
                 tau = t_final - t_now;
