@@ -33,10 +33,10 @@ SOURCES = ["cufsp_common.cu", "cufsp_rtc.cu", "cufsp_kron.cu", "cufsp_kron_plane
            "cufsp_vec.cu", "cufsp_bdf.cu", "cufsp_batch.cu", "cufsp_adjoint.cu", "cufsp_adaptive.cu",
            "cufsp_arnoldi.cu"]
 HEADERS = ["cufsp_internal.h", "cufsp_reduce.cuh", "cufsp_march.h", "cufsp_vec.h", "cufsp_plane.cuh", "cufsp_batch.cuh",
-           "cufsp_sparse_rtc.cuh"]
+           "cufsp_sparse_rtc.cuh", "cufsp_kron_rtc.cuh"]
 # Kernel sources compiled at run time by NVRTC are embedded in the library as string literals.
 RTC_SOURCES = {"cufsp_plane.cuh": "cufsp_plane_src.inc", "cufsp_batch.cuh": "cufsp_batch_src.inc",
-               "cufsp_sparse_rtc.cuh": "cufsp_sparse_src.inc"}
+               "cufsp_sparse_rtc.cuh": "cufsp_sparse_src.inc", "cufsp_kron_rtc.cuh": "cufsp_kron_rtc_src.inc"}
 LINK_LIBS = ["-L/usr/local/cuda/lib64", "-lnvrtc", "-Xlinker", "-rpath,/usr/local/cuda/lib64"]
 
 

@@ -26,7 +26,11 @@
 #include <cstdlib>
 #include <cstring>
 
+#include <sstream>
+
 #include "cufsp_internal.h"
+#define CUFSP_KRON_RTC_MAX_R 64
+#include "cufsp_kron_rtc.cuh"
 #include "cufsp_march.h"
 
 namespace cufsp {
@@ -311,6 +315,11 @@ struct KronData {
     // runtime-specialised plane kernel (cufsp_kron_plane.cu), when the network has its shape
     PlaneData *plane = nullptr;
     std::string plane_why;
+    // kernel specialised for the network and box (cufsp_kron_rtc.cuh), for the other networks
+    std::shared_ptr<RtcModule> rtc;
+    double *d_rtc_tab = nullptr;  // packed tabulated factors
+    int rtc_grid = 0;
+    std::string rtc_why;
 };
 
 // Outer factor table for the inner split k: G[q][r] = (prod_{s>=k} f_{r,s}(x_s - nu_{r,s}), or 0
@@ -458,6 +467,105 @@ static void plan_march(const ModelHost &m, KronData *kd) {
 }
 
 using KronKernel = void (*)(const KronArgs, const double *, double *);
+
+namespace {
+const char *kKronRtcSource =
+#include "cufsp_kron_rtc_src.inc"
+    ;
+int env_or(const char *name, int dflt) {
+    const char *v = getenv(name);
+    return v ? atoi(v) : dflt;
+}
+}  // namespace
+
+// Compiles the KRONECKER kernel specialised for this network and box (cufsp_kron_rtc.cuh): the kind
+// of every factor (ones, identity, table), the packed tables it reads, the shifts and the box as
+// constants.  Sets kd->rtc, or the reason in kd->rtc_why.
+static void kron_build_rtc(const ModelHost &m, KronData *kd) {
+    if (env_or("CUFSP_KRON_RTC", 1) == 0) {
+        kd->rtc_why = "disabled (CUFSP_KRON_RTC=0)";
+        return;
+    }
+    if (m.nr > CUFSP_KRON_RTC_MAX_R) {
+        kd->rtc_why = "more than 64 reactions";
+        return;
+    }
+    const int ns = m.ns, nr = m.nr;
+    std::vector<int> kind((size_t)nr * ns, 0), toff((size_t)nr * ns, 0);
+    std::vector<double> packed;
+    for (int r = 0; r < nr; ++r)
+        for (int s = 0; s < ns; ++s) {
+            const double *t = m.tables.data() + (size_t)r * m.tab_stride + m.tab_off[s];
+            bool ones = true, ident = true;
+            for (int x = 0; x <= m.bounds[s]; ++x) {
+                if (t[x] != 1.0) ones = false;
+                if (t[x] != (double)x) ident = false;
+            }
+            const size_t k = (size_t)r * ns + s;
+            kind[k] = ones ? 0 : (ident ? 1 : 2);
+            if (kind[k] == 2) {
+                toff[k] = (int)packed.size();
+                packed.insert(packed.end(), t, t + m.bounds[s] + 1);
+            }
+        }
+    std::vector<int64_t> stride(ns);
+    int64_t st = 1;
+    for (int s = 0; s < ns; ++s) {
+        stride[s] = st;
+        st *= (int64_t)m.bounds[s] + 1;
+    }
+    const int chunk = std::max(1, std::min(nr, env_or("CUFSP_KRON_RTC_CHUNK", 5)));
+    const int minb = std::max(1, std::min(8, env_or("CUFSP_KRON_RTC_MINB", 2)));
+    const bool tab_smem = packed.size() * sizeof(double) <= 40960;
+    std::ostringstream o;
+    o << "#define CUFSP_KRON_MINB " << minb << "\n#define CUFSP_KRON_RTC_MAX_R " << CUFSP_KRON_RTC_MAX_R
+      << "\n#define CUFSP_KRON_NS " << ns << "\n#define CUFSP_KRON_NR " << nr << "\n#define CUFSP_KRON_N " << m.n
+      << "LL\n#define CUFSP_KRON_CHUNK " << chunk << "\n#define CUFSP_KRON_TS " << std::max<size_t>(1, packed.size())
+      << "\n#define CUFSP_KRON_TAB_SMEM " << (tab_smem ? 1 : 0) << "\nnamespace cufsp_kron {\n";
+    o << "__device__ __forceinline__ constexpr int ext(int s) {";
+    for (int s = 0; s < ns; ++s) o << " if (s == " << s << ") return " << m.bounds[s] + 1 << ";";
+    o << " return 1; }\n";
+    auto emit2 = [&](const char *name, const std::vector<int> &v) {
+        o << "__device__ __forceinline__ constexpr int " << name << "(int r, int s) {";
+        for (int r = 0; r < nr; ++r)
+            for (int s = 0; s < ns; ++s)
+                if (v[(size_t)r * ns + s] != 0)
+                    o << " if (r == " << r << " && s == " << s << ") return " << v[(size_t)r * ns + s] << ";";
+        o << " return 0; }\n";
+    };
+    emit2("nu", m.nu);
+    emit2("kind", kind);
+    emit2("t_off", toff);
+    o << "__device__ __forceinline__ constexpr long long shift(int r) {";
+    for (int r = 0; r < nr; ++r) {
+        int64_t d = 0;
+        for (int s = 0; s < ns; ++s) d += (int64_t)m.nu[(size_t)r * ns + s] * stride[s];
+        o << " if (r == " << r << ") return " << d << "LL;";
+    }
+    o << " return 0; }\n}\n";
+    std::string why;
+    auto mod = rtc_module(o.str() + kKronRtcSource, {"cufsp_kron_mv_accum", "cufsp_kron_mv_set"}, why);
+    if (!mod) {
+        kd->rtc_why = why;
+        return;
+    }
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, (const void *)mod->kernels[0], 256, 0) != cudaSuccess ||
+        occ < 1) {
+        cudaGetLastError();
+        kd->rtc_why = "specialised kernel does not fit an SM";
+        return;
+    }
+    if (packed.empty()) packed.push_back(0.0);
+    if (dev_malloc(&kd->d_rtc_tab, sizeof(double) * packed.size()) != cudaSuccess ||
+        cudaMemcpy(kd->d_rtc_tab, packed.data(), sizeof(double) * packed.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaGetLastError();
+        kd->rtc_why = "table allocation failed";
+        return;
+    }
+    kd->rtc = mod;
+    kd->rtc_grid = device_info().sm_count * occ;
+}
 
 template <int NR, int V>
 static KronKernel pick_ng(int NG, bool accum) {
@@ -631,6 +739,7 @@ cufsp_status kron_create(const ModelHost &m, KronData **out) {
         return cuda_error(e, "kron_create");
     }
     kd->plane = plane_create(m, kd->d_tables, kd->plane_why);
+    kron_build_rtc(m, kd);
     plan_march(m, kd);
     if (kd->march && kd->ma.k != kd->k) {  // the marching split needs its own outer table
         const std::vector<double2> gm = outer_table(m, kd, kd->ma.k);
@@ -650,6 +759,7 @@ void kron_destroy(KronData *k) {
     if (k->d_nu) cudaFree(k->d_nu);
     if (k->d_gtab) cudaFree(k->d_gtab);
     if (k->d_gtab_march) cudaFree(k->d_gtab_march);
+    if (k->d_rtc_tab) cudaFree(k->d_rtc_tab);
     watch_word_free(k->h_err);
     plane_destroy(k->plane);
     delete k;
@@ -671,8 +781,12 @@ cufsp_status kron_prepare(KronData *k, const double *coefs, cudaStream_t st) {
 
 std::string kron_describe(const KronData *k) {
     if (k->plane) return plane_description(k->plane);
+    if (k->rtc)
+        return "kernel specialised for the network and box (NVRTC, sm_100a), " + std::to_string(k->rtc_grid) +
+               " CTAs x 256 threads; plane kernel not used: " + k->plane_why;
     return "k_kron_mv (NR=" + std::to_string(k->NR) + " NG=" + std::to_string(k->NG) + " V=" + std::to_string(k->V) +
-           " inner species=" + std::to_string(k->k) + "); plane kernel not used: " + k->plane_why;
+           " inner species=" + std::to_string(k->k) + "); plane kernel not used: " + k->plane_why +
+           "; specialised kernel not used: " + k->rtc_why;
 }
 
 // ---- transposed action (adjoint solves) ---------------------------------------------------------
@@ -772,6 +886,24 @@ cufsp_status kron_apply(KronData *kd, const double *coefs, double alpha, const d
             CUFSP_CUDA_TRY(cudaGetLastError());
             return CUFSP_SUCCESS;
         }
+    }
+    if (kd->rtc && ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) % 16) == 0) {
+        if (i_end < 0) i_end = kd->n;
+        if (i_end <= i_begin) return CUFSP_SUCCESS;
+        CufspKronRtcArgs r;
+        std::memset(&r, 0, sizeof(r));
+        r.tables = kd->d_rtc_tab;
+        r.d_alpha = d_alpha;
+        r.d_skip = d_skip;
+        r.i_begin = i_begin;
+        r.i_end = i_end;
+        for (int k = 0; k < kd->nr; ++k) r.coef[k] = alpha * coefs[k];
+        const int64_t pairs = (i_end - (i_begin & ~(int64_t)1) + 1) / 2;
+        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(kd->rtc_grid, (pairs + 255) / 256));
+        void *args[] = {&r, (void *)&x, (void *)&y};
+        CUFSP_CUDA_TRY(cudaLaunchKernel((const void *)kd->rtc->kernels[accumulate ? 0 : 1], dim3(grid), dim3(256), args,
+                                        0, st));
+        return CUFSP_SUCCESS;
     }
     KronArgs a;
     a.tables = kd->d_tables;

@@ -160,3 +160,54 @@ def test_plane_kernel_is_deterministic(cuda):
     A.apply(x, y1, coefs=m.coefs(0.0), beta=0.0)
     A.apply(x, y2, coefs=m.coefs(0.0), beta=0.0)
     assert np.array_equal(host(y1), host(y2))
+
+
+def check_general(m, x=None):
+    """A KRONECKER generator not served by the plane kernel against the oracle (both forms)."""
+    A = FSPMat.from_model(m, MatrixFormat.KRONECKER)
+    csr = oracle.assemble_model(m)
+    rng = np.random.default_rng(12)
+    x = rng.uniform(0, 1, m.n_states) if x is None else x
+    y0 = rng.uniform(-1, 1, m.n_states)
+    c = m.coefs(0.0)
+    scale = csr.abs_spmv(c, x).max()
+    for beta in (0.0, 1.0):
+        y = dev(y0)
+        A.apply(dev(x), y, coefs=c, beta=beta)
+        ref = csr.spmv(c, x, y0 if beta else None, beta=beta)
+        err = np.abs(host(y) - ref).max()
+        assert err <= MATVEC_RTOL * (scale + (np.abs(y0).max() if beta else 0.0)), (m.name, m.bounds, beta, err)
+    return A
+
+
+@pytest.mark.parametrize("case", ["gene", "odd_states", "big_change", "random5", "toggle_no_plane"])
+def test_specialised_general_kernel_matches_oracle(cuda, case, monkeypatch):
+    """Networks outside the plane kernel's shape use the KRONECKER kernel specialised per network and
+    box (factor kinds ones / identity / table as constants): 5 species, an odd state count, a change
+    of 2 molecules, random 4-species networks, and a plane-shaped network with the plane kernel off."""
+    if case == "gene":
+        m = models.gene_expression((1, 1, 1, 63, 40), time_varying=False)
+    elif case == "odd_states":
+        m = models.mass_action_3(bounds=(6, 8, 4))  # 7 * 9 * 5 = 315 states, a change of 2 molecules
+        m.nu[0, 0] = 2
+    elif case == "big_change":
+        m = random_network((9, 7, 11), 5, 4)
+        m.nu[1, 2] = -2
+        m.nu[3, 0] = 3
+    elif case == "random5":
+        m = random_network((3, 4, 2, 5, 6), 7, 9)
+    else:
+        monkeypatch.setenv("CUFSP_PLANE", "0")
+        m = models.toggle((63, 40))
+    A = check_general(m)
+    assert "specialised" in A.describe(), A.describe()
+
+
+def test_generic_kernel_remains(cuda, monkeypatch):
+    """With the specialised kernels switched off the generic k_kron_mv serves the generator, to the
+    same bar."""
+    monkeypatch.setenv("CUFSP_KRON_RTC", "0")
+    monkeypatch.setenv("CUFSP_PLANE", "0")
+    for m in (models.gene_expression((1, 1, 1, 40, 23), time_varying=False), models.mass_action_3(bounds=(20, 9, 9))):
+        A = check_general(m)
+        assert "k_kron_mv" in A.describe(), A.describe()
