@@ -351,6 +351,36 @@ def sparse_secondary(steps: int = 200) -> dict:
             "frac_of_hbm_peak": round(gbs / peak, 4), "kernel": A.describe()}
 
 
+def kron_general_secondary(steps: int = 200) -> dict:
+    """The KRONECKER action of the 5-species gene network on an HBM-sized box (1,1,1,127,8191) =
+    8,388,608 states, outside the plane kernel's shape, through the kernel specialised per network and
+    box: y += A x over 2 rotating (x, y) pairs (268 MB > L2), CUDA events, 24 B/state."""
+    import torch
+    from cuda_fsp_b200 import FSPMat, MatrixFormat, models
+    m = models.gene_expression((1, 1, 1, 127, 8191), time_varying=False)
+    n = m.n_states
+    A = FSPMat.from_model(m, MatrixFormat.KRONECKER)
+    g = torch.Generator(device="cuda").manual_seed(6)
+    xs = [torch.rand(n, dtype=torch.float64, device="cuda", generator=g) for _ in range(2)]
+    ys = [torch.zeros(n, dtype=torch.float64, device="cuda") for _ in range(2)]
+    c = m.coefs(0)
+    for i in range(4):
+        A.apply(xs[i % 2], ys[i % 2], coefs=c, beta=1.0)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for i in range(steps):
+        A.apply(xs[i % 2], ys[i % 2], coefs=c, beta=1.0)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    gbs = BYTES_PER_STATE * n / (ms * 1e-3) / 1e9
+    peak, _ = measured_peak_hbm()
+    return {"metric": "KRONECKER matvec GB/s (general networks)", "workload": "gene_expression 5 species, box "
+            "1x1x1x127x8191 = 8,388,608 states, 12 reactions, y += A x", "value": round(gbs, 1),
+            "us_per_action": round(ms * 1e3, 2), "frac_of_hbm_peak": round(gbs / peak, 4), "kernel": A.describe()}
+
+
 def bdf_secondary() -> dict:
     """BDF leg: the time-varying gene-expression model (131,072 states, switching rate
     k0 sigmoid((t - 5) / 0.5)) from p0 to t = 60 by the device BDF integrator (rtol 1e-8, atol 1e-14;
@@ -612,7 +642,7 @@ def run_ours(args):
     elif rank == 0:
         secondary = expmv_secondary()
         secondary["cpu_oracle_ms_per_solve"] = round(cpu_expmv_ms(), 1)
-        secondary = [secondary, sparse_secondary(), bdf_secondary(), expmv_large_secondary(), batched_secondary(),
+        secondary = [secondary, sparse_secondary(), kron_general_secondary(), bdf_secondary(), expmv_large_secondary(), batched_secondary(),
                      gradient_secondary()]
     cpu = cpu_oracle_gbs(max(3, min(args.steps, 20)), 3) if (rank == 0 and world == 1) else None
     peak, peak_kind = measured_peak_hbm()
