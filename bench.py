@@ -674,6 +674,8 @@ def run_ours(args):
 def run_leg(args):
     """One leg alone, for profiling its kernels under ncu (small steps, one JSON line, no extras):
       sparse  the CSR/HYB generator action y += A x on mass_action_3 (--box, default 255^3)
+      kgen    the KRONECKER action of the 5-species gene network (--box, default 1,1,1,127,8191): the
+              specialised general kernel
       krylov  Krylov steps exp(tA)p0 on mass_action_3 (--box; above 2^20 states the launch sequence
               of plane-kernel matvecs and the k_mdot / k_mupd / k_comb vector kernels)
       adjoint one log-likelihood gradient on the gene model (--box, default 1,1,1,127,127)
@@ -705,6 +707,24 @@ def run_leg(args):
         bps = 24 + 8 * m.nr
         out.update({"n_states": m.n_states, "us_per_action": round(ms * 1e3, 2), "bytes_per_state": bps,
                     "gbs": round(bps * m.n_states / (ms * 1e-3) / 1e9, 1), "kernel": A.describe()})
+    elif args.leg == "kgen":
+        m = models.gene_expression(tuple(box) if box else (1, 1, 1, 127, 8191), time_varying=False)
+        A = FSPMat.from_model(m, MatrixFormat.KRONECKER)
+        g = torch.Generator(device="cuda").manual_seed(6)
+        xs = [torch.rand(m.n_states, dtype=torch.float64, device="cuda", generator=g) for _ in range(2)]
+        ys = [torch.zeros(m.n_states, dtype=torch.float64, device="cuda") for _ in range(2)]
+        c = m.coefs(0)
+        for i in range(max(3, args.warmup)):
+            A.apply(xs[i % 2], ys[i % 2], coefs=c, beta=1.0)
+        torch.cuda.synchronize()
+        ev0.record()
+        for i in range(args.steps):
+            A.apply(xs[i % 2], ys[i % 2], coefs=c, beta=1.0)
+        ev1.record()
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1) / args.steps
+        out.update({"n_states": m.n_states, "us_per_action": round(ms * 1e3, 2),
+                    "gbs": round(BYTES_PER_STATE * m.n_states / (ms * 1e-3) / 1e9, 1), "kernel": A.describe()})
     elif args.leg == "krylov":
         m = models.mass_action_3(bounds=box) if box else models.mass_action_3()
         A = FSPMat.from_model(m, MatrixFormat.KRONECKER)
@@ -782,7 +802,7 @@ def main():
     ap.add_argument("--sets", type=int, default=4, help="rotating (x, y) input pairs; parameter sets of the gradbatch leg")
     ap.add_argument("--no-extras", action="store_true",
                     help="time the generator action only (no e2e, expmv or CPU legs); for profiling runs")
-    ap.add_argument("--leg", choices=["sparse", "krylov", "adjoint", "gradbatch", "bdf", "states"], default=None,
+    ap.add_argument("--leg", choices=["sparse", "kgen", "krylov", "adjoint", "gradbatch", "bdf", "states"], default=None,
                     help="run one leg alone (profiling runs; see run_leg)")
     ap.add_argument("--box", default=None, help="box bounds of the leg, comma separated")
     ap.add_argument("--workers", type=int, default=2, help="host workers of the gradbatch leg")
