@@ -320,6 +320,8 @@ struct KronData {
     double *d_rtc_tab = nullptr;  // packed tabulated factors
     int rtc_grid = 0;
     std::string rtc_why;
+    bool rtc_tried = false;       // built at create without a plane kernel, else at first need
+    const ModelHost *model = nullptr;  // the generator's model (outlives this object), for the lazy build
 };
 
 // Outer factor table for the inner split k: G[q][r] = (prod_{s>=k} f_{r,s}(x_s - nu_{r,s}), or 0
@@ -482,6 +484,7 @@ int env_or(const char *name, int dflt) {
 // of every factor (ones, identity, table), the packed tables it reads, the shifts and the box as
 // constants.  Sets kd->rtc, or the reason in kd->rtc_why.
 static void kron_build_rtc(const ModelHost &m, KronData *kd) {
+    kd->rtc_tried = true;
     if (env_or("CUFSP_KRON_RTC", 1) == 0) {
         kd->rtc_why = "disabled (CUFSP_KRON_RTC=0)";
         return;
@@ -544,7 +547,8 @@ static void kron_build_rtc(const ModelHost &m, KronData *kd) {
     }
     o << " return 0; }\n}\n";
     std::string why;
-    auto mod = rtc_module(o.str() + kKronRtcSource, {"cufsp_kron_mv_accum", "cufsp_kron_mv_set"}, why);
+    auto mod = rtc_module(o.str() + kKronRtcSource, {"cufsp_kron_mv_accum", "cufsp_kron_mv_set", "cufsp_kron_mvT_set"},
+                          why);
     if (!mod) {
         kd->rtc_why = why;
         return;
@@ -739,7 +743,8 @@ cufsp_status kron_create(const ModelHost &m, KronData **out) {
         return cuda_error(e, "kron_create");
     }
     kd->plane = plane_create(m, kd->d_tables, kd->plane_why);
-    kron_build_rtc(m, kd);
+    kd->model = &m;
+    if (!kd->plane) kron_build_rtc(m, kd);  // with a plane kernel, only ranges it declines need it
     plan_march(m, kd);
     if (kd->march && kd->ma.k != kd->k) {  // the marching split needs its own outer table
         const std::vector<double2> gm = outer_table(m, kd, kd->ma.k);
@@ -839,6 +844,21 @@ __global__ void __launch_bounds__(256) k_kron_mvT(const KronTArgs a, const doubl
 
 cufsp_status kron_apply_transpose(KronData *kd, const double *coefs, double alpha, const double *d_alpha,
                                   const int *d_skip, const double *x, double *y, cudaStream_t st) {
+    if (!kd->rtc_tried && kd->model) kron_build_rtc(*kd->model, kd);
+    if (kd->rtc && ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) % 16) == 0) {
+        CufspKronRtcArgs r;
+        std::memset(&r, 0, sizeof(r));
+        r.tables = kd->d_rtc_tab;
+        r.d_alpha = d_alpha;
+        r.d_skip = d_skip;
+        r.i_begin = 0;
+        r.i_end = kd->n;
+        for (int k = 0; k < kd->nr; ++k) r.coef[k] = alpha * coefs[k];
+        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(kd->rtc_grid, (kd->n / 2 + 256) / 256));
+        void *args[] = {&r, (void *)&x, (void *)&y};
+        CUFSP_CUDA_TRY(cudaLaunchKernel((const void *)kd->rtc->kernels[2], dim3(grid), dim3(256), args, 0, st));
+        return CUFSP_SUCCESS;
+    }
     KronTArgs a;
     std::memset(&a, 0, sizeof(a));
     a.tables = kd->d_tables;
@@ -887,6 +907,7 @@ cufsp_status kron_apply(KronData *kd, const double *coefs, double alpha, const d
             return CUFSP_SUCCESS;
         }
     }
+    if (!kd->rtc_tried && kd->model) kron_build_rtc(*kd->model, kd);
     if (kd->rtc && ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) % 16) == 0) {
         if (i_end < 0) i_end = kd->n;
         if (i_end <= i_begin) return CUFSP_SUCCESS;

@@ -15,7 +15,8 @@
 // the CTA stages the tables it needs (through L1 when they exceed 40 KB).  Each thread owns one aligned pair of states (i, i + 1), i
 // even: x[i..i+1] and y[i..i+1] are 16-byte accesses, and the sources of a reaction with an even
 // shift d_r are one 16-byte load (two 8-byte loads for an odd shift).  The gathers of a chunk of
-// reactions are issued before their first use.
+// reactions are issued before their first use.  The transposed operator (adjoint solves) is the same
+// pass with the propensity at the state and the gather at x + nu_r.
 #ifndef CUFSP_KRON_RTC_CUH
 #define CUFSP_KRON_RTC_CUH
 
@@ -93,13 +94,32 @@ __device__ __forceinline__ void propensities(const double *tab, const State &st,
     src = ok ? sv : 0.0;
 }
 
+// Transposed generator (adjoint solves): (A^T l)(x) = sum_r c_r a_r(x) (l[x + nu_r] 1{x + nu_r in box}
+// - l[x]): the propensity at the state, the gather at x + nu_r.
+template <int R>
+__device__ __forceinline__ void propensities_t(const double *tab, const State &st, double &diag, double &dst) {
+    double d = 1.0;
+    bool ok = true;
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+        const int v = st.x[s];
+        if (nu(R, s) != 0) {
+            const int w = v + nu(R, s);
+            ok = ok && w >= 0 && w < ext(s);
+        }
+        if (kind(R, s) != 0) d *= factor<R>(tab, s, v);
+    }
+    diag = d;
+    dst = ok ? d : 0.0;
+}
+
 struct Pending {
     double xs0, xs1;  // x at the two sources
 };
 
-template <int R>
+template <int R, bool TRANS>
 __device__ __forceinline__ void load_reaction(const double *__restrict__ x, long long i, bool pair, Pending &q) {
-    constexpr long long D = shift(R);
+    constexpr long long D = TRANS ? -shift(R) : shift(R);
     const long long s0 = clamp_index(i - D), s1 = clamp_index(i + 1 - D);
     if constexpr ((D & 1) == 0) {
         if (pair && s1 == s0 + 1) {  // sources of an even shift are an aligned pair
@@ -113,44 +133,49 @@ __device__ __forceinline__ void load_reaction(const double *__restrict__ x, long
     q.xs1 = pair ? __ldg(x + s1) : 0.0;
 }
 
-template <int R0, int R>
+template <int R0, int R, bool TRANS>
 __device__ __forceinline__ void load_chunk(const double *__restrict__ x, long long i, bool pair, Pending (&q)[CHUNK]) {
     if constexpr (R < NR && R < R0 + CHUNK) {
-        load_reaction<R>(x, i, pair, q[R - R0]);
-        load_chunk<R0, R + 1>(x, i, pair, q);
+        load_reaction<R, TRANS>(x, i, pair, q[R - R0]);
+        load_chunk<R0, R + 1, TRANS>(x, i, pair, q);
     }
 }
 
-template <int R0, int R>
+template <int R0, int R, bool TRANS>
 __device__ __forceinline__ void accumulate_chunk(const CufspKronRtcArgs &a, const double *tab, const State &s0,
                                                  const State &s1, const Pending (&q)[CHUNK], double (&d)[2],
                                                  double (&o)[2]) {
     if constexpr (R < NR && R < R0 + CHUNK) {
         const double c = a.coef[R];
         double d0, f0, d1, f1;
-        propensities<R>(tab, s0, d0, f0);
-        propensities<R>(tab, s1, d1, f1);
+        if constexpr (TRANS) {
+            propensities_t<R>(tab, s0, d0, f0);
+            propensities_t<R>(tab, s1, d1, f1);
+        } else {
+            propensities<R>(tab, s0, d0, f0);
+            propensities<R>(tab, s1, d1, f1);
+        }
         d[0] = fma(c, d0, d[0]);
         d[1] = fma(c, d1, d[1]);
         o[0] = fma(c, f0 * q[R - R0].xs0, o[0]);
         o[1] = fma(c, f1 * q[R - R0].xs1, o[1]);
-        accumulate_chunk<R0, R + 1>(a, tab, s0, s1, q, d, o);
+        accumulate_chunk<R0, R + 1, TRANS>(a, tab, s0, s1, q, d, o);
     }
 }
 
-template <int R0>
+template <int R0, bool TRANS>
 __device__ __forceinline__ void all_reactions(const CufspKronRtcArgs &a, const double *tab,
                                               const double *__restrict__ x, long long i, bool pair, const State &s0,
                                               const State &s1, double (&d)[2], double (&o)[2]) {
     if constexpr (R0 < NR) {
         Pending q[CHUNK];
-        load_chunk<R0, R0>(x, i, pair, q);
-        accumulate_chunk<R0, R0>(a, tab, s0, s1, q, d, o);
-        all_reactions<R0 + CHUNK>(a, tab, x, i, pair, s0, s1, d, o);
+        load_chunk<R0, R0, TRANS>(x, i, pair, q);
+        accumulate_chunk<R0, R0, TRANS>(a, tab, s0, s1, q, d, o);
+        all_reactions<R0 + CHUNK, TRANS>(a, tab, x, i, pair, s0, s1, d, o);
     }
 }
 
-template <bool ACCUM>
+template <bool ACCUM, bool TRANS>
 __device__ __forceinline__ void kron_mv(const CufspKronRtcArgs &a, const double *__restrict__ x, double *__restrict__ y) {
 #if CUFSP_KRON_TAB_SMEM
     __shared__ double tab[TS];
@@ -180,7 +205,7 @@ __device__ __forceinline__ void kron_mv(const CufspKronRtcArgs &a, const double 
         const State s0 = decode((unsigned)i);
         const State s1 = decode((unsigned)(pair ? i + 1 : i));
         double d[2] = {0.0, 0.0}, o[2] = {0.0, 0.0};
-        all_reactions<0>(a, tab, x, i, pair, s0, s1, d, o);
+        all_reactions<0, TRANS>(a, tab, x, i, pair, s0, s1, d, o);
         double r0 = alpha * fma(-d[0], xv.x, o[0]);
         double r1 = alpha * fma(-d[1], xv.y, o[1]);
         if (ACCUM) {
@@ -202,13 +227,20 @@ __device__ __forceinline__ void kron_mv(const CufspKronRtcArgs &a, const double 
 extern "C" __global__ void __launch_bounds__(256, CUFSP_KRON_MINB) cufsp_kron_mv_accum(const CufspKronRtcArgs a,
                                                                                       const double *__restrict__ x,
                                                                                       double *__restrict__ y) {
-    cufsp_kron::kron_mv<true>(a, x, y);
+    cufsp_kron::kron_mv<true, false>(a, x, y);
 }
 
 extern "C" __global__ void __launch_bounds__(256, CUFSP_KRON_MINB) cufsp_kron_mv_set(const CufspKronRtcArgs a,
                                                                                     const double *__restrict__ x,
                                                                                     double *__restrict__ y) {
-    cufsp_kron::kron_mv<false>(a, x, y);
+    cufsp_kron::kron_mv<false, false>(a, x, y);
+}
+
+// y = alpha * A^T x (overwrite): the adjoint solves' operator.
+extern "C" __global__ void __launch_bounds__(256, CUFSP_KRON_MINB) cufsp_kron_mvT_set(const CufspKronRtcArgs a,
+                                                                                     const double *__restrict__ x,
+                                                                                     double *__restrict__ y) {
+    cufsp_kron::kron_mv<false, true>(a, x, y);
 }
 
 #endif  // __CUDACC_RTC__

@@ -127,3 +127,35 @@ def test_torch_autograd_wrapper(cuda):
     ll_ref, g_ref = L.gradient(np.exp(lt.detach().numpy()))  # the same rates, bit for bit
     assert abs(ll.item() - ll_ref) <= 1e-12 * abs(ll_ref)
     assert np.max(np.abs(lt.grad.numpy() - g_ref)) <= 1e-9 * np.max(np.abs(g_ref))
+
+
+def test_adjoint_through_the_launch_sequence(cuda):
+    """The gradient with the multi-launch Arnoldi pass (the path of generators above the persistent
+    pass's size: the transposed generator action is the specialised kernel's A^T pass), run in a child
+    process with CUFSP_ARNOLDI_PERSISTENT=0, against forward sensitivities."""
+    import json
+    import os
+    import subprocess
+    import sys
+    from pathlib import Path
+    root = Path(__file__).resolve().parent.parent
+    code = (
+        "import json, numpy as np, sys; sys.path.insert(0, %r)\n"
+        "from cuda_fsp_b200 import Likelihood, models\n"
+        "m = models.gene_expression((1, 1, 1, 15, 15), time_varying=False)\n"
+        "times = np.geomspace(1.0, 60.0, 8)\n"
+        "counts = np.random.default_rng(1).integers(0, 4, size=(8, m.n_states // 8)).astype(float)\n"
+        "L = Likelihood(m, times, counts, n_marginal=3, kry_tol=1e-10)\n"
+        "ll, g = L.gradient()\n"
+        "print(json.dumps({'ll': ll, 'g': list(g), 'kernel': L.A.describe()}))\n" % str(root))
+    env = dict(os.environ, CUFSP_ARNOLDI_PERSISTENT="0")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600, env=env)
+    assert r.returncode == 0, r.stdout + r.stderr
+    out = json.loads(r.stdout.strip().splitlines()[-1])
+    m = models.gene_expression((1, 1, 1, 15, 15), time_varying=False)
+    times = np.geomspace(1.0, 60.0, 8)
+    counts = np.random.default_rng(1).integers(0, 4, size=(8, m.n_states // 8)).astype(float)
+    ll_ref, g_ref = oracle.loglik_grad_forward(oracle.assemble_model(m), m.coefs(0), times, m.p0(), counts, 8)
+    assert "specialised" in out["kernel"], out["kernel"]
+    assert abs(out["ll"] - ll_ref) <= 1e-8 * abs(ll_ref)
+    assert rel_err(np.array(out["g"]), g_ref) <= GRAD_RTOL, (out["g"], g_ref)
