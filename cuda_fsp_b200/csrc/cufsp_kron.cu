@@ -320,7 +320,8 @@ struct KronData {
     double *d_rtc_tab = nullptr;  // packed tabulated factors
     int rtc_grid = 0;
     std::string rtc_why;
-    bool rtc_tried = false;       // built at create without a plane kernel, else at first need
+    bool rtc_tried = false;       // built at the first transposed action (or at create when it serves the forward)
+    bool rtc_forward = false;     // CUFSP_KRON_RTC=1: it also serves the forward action
     const ModelHost *model = nullptr;  // the generator's model (outlives this object), for the lazy build
 };
 
@@ -485,7 +486,7 @@ int env_or(const char *name, int dflt) {
 // constants.  Sets kd->rtc, or the reason in kd->rtc_why.
 static void kron_build_rtc(const ModelHost &m, KronData *kd) {
     kd->rtc_tried = true;
-    if (env_or("CUFSP_KRON_RTC", 1) == 0) {
+    if (env_or("CUFSP_KRON_RTC", -1) == 0) {
         kd->rtc_why = "disabled (CUFSP_KRON_RTC=0)";
         return;
     }
@@ -744,7 +745,12 @@ cufsp_status kron_create(const ModelHost &m, KronData **out) {
     }
     kd->plane = plane_create(m, kd->d_tables, kd->plane_why);
     kd->model = &m;
-    if (!kd->plane) kron_build_rtc(m, kd);  // with a plane kernel, only ranges it declines need it
+    // The specialised kernel serves the transposed action (built at its first use).  For the forward
+    // action it is opt-in (CUFSP_KRON_RTC=1): it recomputes every propensity from the factors per
+    // state, which on the 12-reaction gene network at 8.4M states is issue-bound (1.76 TB/s) where the
+    // generic kernel, sharing inner and outer factor products across a row, moves 1.92 TB/s.
+    kd->rtc_forward = env_or("CUFSP_KRON_RTC", -1) == 1;
+    if (kd->rtc_forward && !kd->plane) kron_build_rtc(m, kd);
     plan_march(m, kd);
     if (kd->march && kd->ma.k != kd->k) {  // the marching split needs its own outer table
         const std::vector<double2> gm = outer_table(m, kd, kd->ma.k);
@@ -786,12 +792,12 @@ cufsp_status kron_prepare(KronData *k, const double *coefs, cudaStream_t st) {
 
 std::string kron_describe(const KronData *k) {
     if (k->plane) return plane_description(k->plane);
-    if (k->rtc)
+    if (k->rtc_forward && k->rtc)
         return "kernel specialised for the network and box (NVRTC, sm_100a), " + std::to_string(k->rtc_grid) +
                " CTAs x 256 threads; plane kernel not used: " + k->plane_why;
     return "k_kron_mv (NR=" + std::to_string(k->NR) + " NG=" + std::to_string(k->NG) + " V=" + std::to_string(k->V) +
            " inner species=" + std::to_string(k->k) + "); plane kernel not used: " + k->plane_why +
-           "; specialised kernel not used: " + k->rtc_why;
+           (k->rtc_forward ? "; specialised kernel not used: " + k->rtc_why : std::string());
 }
 
 // ---- transposed action (adjoint solves) ---------------------------------------------------------
@@ -907,8 +913,9 @@ cufsp_status kron_apply(KronData *kd, const double *coefs, double alpha, const d
             return CUFSP_SUCCESS;
         }
     }
-    if (!kd->rtc_tried && kd->model) kron_build_rtc(*kd->model, kd);
-    if (kd->rtc && ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) % 16) == 0) {
+    if (kd->rtc_forward && !kd->rtc_tried && kd->model) kron_build_rtc(*kd->model, kd);
+    if (kd->rtc_forward && kd->rtc &&
+        ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) % 16) == 0) {
         if (i_end < 0) i_end = kd->n;
         if (i_end <= i_begin) return CUFSP_SUCCESS;
         CufspKronRtcArgs r;

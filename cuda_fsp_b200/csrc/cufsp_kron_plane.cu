@@ -197,10 +197,11 @@ PlaneData *plane_create(const ModelHost &m, const double *d_tables, std::string 
     pd->threads = 32 * chunks;
     pd->pitch = 64 * chunks;
     const int ytma = env_int("CUFSP_PLANE_YTMA", 1) != 0 ? 1 : 0;
+    const int pps = env_int("CUFSP_PLANE_PPS", 1) == 2 ? 2 : 1;  // planes per CTA barrier
     const DeviceInfo &di = device_info();
     const int want_tr = env_int("CUFSP_PLANE_TR", 2);
     const int env_s = env_int("CUFSP_PLANE_STAGES", 0);
-    const int min_s = 3;
+    const int min_s = pps == 2 ? 4 : 3;
     const int max_s = env_s > 0 ? std::max(min_s, std::min(12, env_s)) : 5;
     auto stage_bytes = [&](int tr_, bool accum) {
         const int nq_ = rows ? tr_ + 2 : 1;
@@ -247,7 +248,7 @@ PlaneData *plane_create(const ModelHost &m, const double *d_tables, std::string 
     s << "#define CUFSP_PLANE_NR " << nr << "\n#define CUFSP_PLANE_NOFF " << offs.size() << "\n#define CUFSP_PLANE_NFA "
       << fa_tabs.size() << "\n#define CUFSP_PLANE_NFB " << fb_tabs.size() << "\n#define CUFSP_PLANE_NT " << terms.size()
       << "\n#define CUFSP_PLANE_NDG " << dgs.size() << "\n#define CUFSP_PLANE_TR " << tr << "\n#define CUFSP_PLANE_STAGES "
-      << stages << "\n#define CUFSP_PLANE_YTMA " << ytma << "\n#define CUFSP_PLANE_ROWS " << (rows ? 1 : 0) << "\n#define CUFSP_PLANE_THREADS " << pd->threads
+      << stages << "\n#define CUFSP_PLANE_PPS " << pps << "\n#define CUFSP_PLANE_YTMA " << ytma << "\n#define CUFSP_PLANE_ROWS " << (rows ? 1 : 0) << "\n#define CUFSP_PLANE_THREADS " << pd->threads
       << "\n#define CUFSP_PLANE_MINB " << minb << "\n";
     // Tries of the bounded waits before a plane is computed (tests of the watchdog only).
     if (const char *wt = getenv("CUFSP_PLANE_WAIT_TRIES")) s << "#define CUFSP_PLANE_WAIT_TRIES " << std::max(0, atoi(wt)) << "\n";
@@ -314,7 +315,7 @@ PlaneData *plane_create(const ModelHost &m, const double *d_tables, std::string 
     std::ostringstream d;
     d << "plane kernel (NVRTC, sm_100a, TMA ring): NR=" << nr << " offsets=" << offs.size() << " terms=" << terms.size()
       << " diag groups=" << dgs.size() << " factor slots=" << fa_tabs.size() << "+" << fb_tabs.size() << " TR=" << tr
-      << " stages=" << stages << " ytma=" << ytma << " threads=" << pd->threads << " CTAs/SM=" << pd->occ_accum;
+      << " stages=" << stages << " planes/step=" << pps << " ytma=" << ytma << " threads=" << pd->threads << " CTAs/SM=" << pd->occ_accum;
     pd->description = d.str();
     return pd.release();
 }
@@ -384,15 +385,32 @@ bool plane_launch(PlaneData *pd, const double *coefs, double alpha, const double
     a.z_end = ze;
     a.alpha = alpha;
     a.nwp = pd->wa.nwp;
-    // One wave: as many CTAs as fit the SMs at once, each with an equal share of the plane units
-    // (CUFSP_PLANE_GRID overrides the count, for tuning).
-    const int64_t units = (int64_t)pd->row_blocks * (ze - zb);
+    // Plane segments: fill the resident CTA slots in as few waves as possible, counting the two
+    // extra planes every segment reads around its output planes.
+    const int planes = ze - zb;
     const int64_t slots = (int64_t)device_info().sm_count * (accumulate ? pd->occ_accum : pd->occ_set);
-    int64_t grid = env_int("CUFSP_PLANE_GRID", 0);
-    if (grid <= 0) grid = slots;
-    grid = std::max<int64_t>(1, std::min(grid, units));
+    int nseg = env_int("CUFSP_PLANE_NSEG", 0);
+    if (nseg <= 0) {
+        double best = 1e300;
+        for (int sgs = 1; sgs <= planes; ++sgs) {
+            const int zs = (planes + sgs - 1) / sgs;
+            const int real = (planes + zs - 1) / zs;
+            const int64_t items = (int64_t)pd->row_blocks * real;
+            const double waves = (double)((items + slots - 1) / slots);
+            const double cost = waves * (zs + 2);
+            if (cost < best - 1e-9) {
+                best = cost;
+                nseg = real;
+            }
+            if (items > 8 * slots) break;
+        }
+    }
+    nseg = std::max(1, std::min(nseg, planes));
+    a.zseg = (planes + nseg - 1) / nseg;
+    const int segs = (planes + a.zseg - 1) / a.zseg;
+    a.items = pd->row_blocks * segs;
     void *args[] = {&a, (void *)&x, (void *)&y};
-    cudaError_t e = cudaLaunchKernel((const void *)pd->k->kernels[accumulate ? 0 : 1], dim3((unsigned)grid),
+    cudaError_t e = cudaLaunchKernel((const void *)pd->k->kernels[accumulate ? 0 : 1], dim3((unsigned)a.items),
                                      dim3((unsigned)pd->threads), args, accumulate ? pd->smem_accum : pd->smem_set, st);
     if (e != cudaSuccess) *status = cuda_error(e, "plane kernel launch");
     return true;

@@ -27,13 +27,11 @@
 //  * Row words (c_r x outer factor, merged per term / diagonal group) come from a table the host
 //    rebuilds when the coefficients change (cufsp_kron_plane.cu), staged with the plane; one CTA
 //    barrier per plane releases the stage.
-//  * One wave of CTAs (the grid is the resident CTA slots): CTA b takes an equal share of the
-//    (row block, plane) units, one or two segments of consecutive planes, and its TMA ring runs on
-//    from one segment into the next; a stage is refilled as soon as the CTA is done with its plane.
 //  * Every mbarrier wait is bounded.  On expiry the CTA records an error in *err, waits (bounded)
 //    for its own copies still in flight, and returns; no CTA exits with a copy outstanding.
-//  * Halo rows and planes outside the box copy the nearest row / plane of the box: finite values
-//    that meet zero coefficients.
+//  * Rows outside the box are never copied: their stage rows are zeroed once and their
+//    coefficients are zero.  Planes outside the box copy the nearest plane (finite values that
+//    meet zero coefficients).
 // x and y must be 16-byte aligned and n0 even (pairs); the host checks both.
 
 #ifndef CUFSP_PLANE_CUH
@@ -53,8 +51,9 @@ struct CufspPlaneArgs {
     int tab_stride;
     int pitch;             // doubles per staged row (n0 rounded up to 64)
     int row_blocks;        // n1 / TR
-    int z_begin, z_end;    // planes to compute; CTA b takes plane units [U b / grid, U (b + 1) / grid),
-                           // U = row_blocks * (z_end - z_begin), row block major
+    int zseg;              // planes per segment
+    int z_begin, z_end;    // planes to compute
+    int items;             // row_blocks * segments = CTAs
     int nwp;               // words per row, padded to even
     double alpha;          // scale of every coefficient (times *d_alpha)
 };
@@ -71,6 +70,8 @@ constexpr int NT = CUFSP_PLANE_NT;      // shifted terms (offset, factor slot)
 constexpr int NDG = CUFSP_PLANE_NDG;    // diagonal groups (factor slot or constant 1)
 constexpr int TR = CUFSP_PLANE_TR;      // tile rows
 constexpr int S = CUFSP_PLANE_STAGES;   // ring stages
+constexpr int PPS = CUFSP_PLANE_PPS;    // planes per CTA barrier (1 or 2)
+static_assert(PPS == 1 || (PPS == 2 && S >= 4), "two planes per step need at least 4 stages");
 constexpr bool ROWS = CUFSP_PLANE_ROWS != 0;
 constexpr bool YTMA = CUFSP_PLANE_YTMA != 0;  // stage y rows in the ring (else L2 prefetch + loads)
 constexpr int NQ = ROWS ? TR + 2 : 1;   // staged x rows per plane (tile + halo)
@@ -138,8 +139,9 @@ struct Layout {
 };
 
 struct Tile {
-    int x1_0;    // first tile row
-    int z0, z1;  // output planes [z0, z1)
+    int x1_0;      // first tile row
+    int rlo, rhi;  // staged x rows [rlo, rhi) of the NQ (rows inside the box)
+    int z0, z1;    // output planes [z0, z1)
 };
 
 // Issue the copies of plane p into its stage (one thread).
@@ -149,13 +151,12 @@ __device__ __forceinline__ void issue_plane(const CufspPlaneArgs &a, const Tile 
     const int pc = min(max(p, 0), a.n2 - 1);
     const bool out = p >= t.z0 && p < t.z1;
     const unsigned row_bytes = (unsigned)a.n0 * 8u;
-    unsigned bytes = (unsigned)NQ * row_bytes;
+    unsigned bytes = (unsigned)(t.rhi - t.rlo) * row_bytes;
     if (out) bytes += (unsigned)Layout<ACCUM>::YR * row_bytes + (unsigned)(TR * NWP * 8);
     mbar_expect_tx(bar, bytes);
     const size_t plane = (size_t)pc * a.n1;
-    for (int i = 0; i < NQ; ++i) {
-        // halo rows outside the box copy the nearest row: finite values that meet zero row words
-        const int x1 = ROWS ? min(max(t.x1_0 - 1 + i, 0), a.n1 - 1) : 0;
+    for (int i = t.rlo; i < t.rhi; ++i) {
+        const int x1 = ROWS ? t.x1_0 - 1 + i : 0;
         tma_load(stage + i * a.pitch, x + (plane + x1) * a.n0, row_bytes, bar);
     }
     if (out) {
@@ -279,56 +280,14 @@ __device__ __forceinline__ void compute_rows(const CufspPlaneArgs &a, const Lane
     }
 }
 
-// A CTA's work is the range [u_begin, u_end) of plane units u = rb * planes + (z - z_begin), row block
-// rb major; the runs of one row block are its segments (one or two, rarely more).  Loads are numbered
-// in the order they are issued across all segments -- for every segment the planes z0 - 1 .. z1 -- and
-// load k uses ring stage k % S with mbarrier parity (k / S) & 1, so the ring flows on from one segment
-// into the next without draining.
-__device__ __forceinline__ void unit_range(const CufspPlaneArgs &a, long long &u_begin, long long &u_end) {
-    const long long units = (long long)a.row_blocks * (a.z_end - a.z_begin);
-    u_begin = units * blockIdx.x / gridDim.x;
-    u_end = units * (blockIdx.x + 1) / gridDim.x;
-}
-
-// Segment j of this CTA's unit range.
-__device__ __forceinline__ Tile segment_of(const CufspPlaneArgs &a, int j) {
-    long long u_begin, u_end;
-    unit_range(a, u_begin, u_end);
-    const long long planes = a.z_end - a.z_begin;
-    const long long rb = u_begin / planes + j;
-    const long long s = j == 0 ? u_begin : rb * planes;
-    const long long e = min(u_end, (rb + 1) * planes);
-    Tile t;
-    t.x1_0 = (int)rb * TR;
-    t.z0 = a.z_begin + (int)(s - rb * planes);
-    t.z1 = a.z_begin + (int)(e - rb * planes);
-    return t;
-}
-
-// State of the thread (0) that issues the copies, kept in shared memory so that it costs the other
-// threads no registers.
-struct Producer {
-    int issued, released;  // loads issued; stages released by the consumers
-    int seg, p;            // segment and plane of the next load
-    Tile t;                // that segment
-};
-
 template <bool ACCUM>
 __device__ __forceinline__ void plane_mv(const CufspPlaneArgs &a, const double *__restrict__ x, double *__restrict__ y) {
     using LY = Layout<ACCUM>;
     extern __shared__ __align__(128) double smem[];
     __shared__ __align__(8) unsigned long long bars[S];
     __shared__ int failed_flag;
-    __shared__ Producer prod;
     if (a.d_skip && *a.d_skip) return;
-    int n_seg;
-    {
-        long long u_begin, u_end;
-        unit_range(a, u_begin, u_end);
-        if (u_begin >= u_end) return;  // whole CTA leaves before any barrier or copy
-        const int planes = a.z_end - a.z_begin;
-        n_seg = (int)((u_end - 1) / planes - u_begin / planes) + 1;
-    }
+    if ((int)blockIdx.x >= a.items) return;
     const int tid = threadIdx.x;
     Lane L;
     L.lane = tid & 31;
@@ -337,9 +296,17 @@ __device__ __forceinline__ void plane_mv(const CufspPlaneArgs &a, const double *
     L.active = L.x0 < a.n0;
     L.has_left = L.warp > 0;
     L.has_right = L.warp * 64 + 64 < a.n0;
+    Tile t;
+    const int rb = blockIdx.x % a.row_blocks, seg = blockIdx.x / a.row_blocks;
+    t.x1_0 = rb * TR;
+    t.z0 = a.z_begin + seg * a.zseg;
+    t.z1 = min(a.z_end, t.z0 + a.zseg);
+    if (t.z0 >= t.z1) return;  // whole CTA leaves before any barrier or copy
+    t.rlo = ROWS ? max(0, 1 - t.x1_0) : 0;
+    t.rhi = ROWS ? min(NQ, a.n1 - t.x1_0 + 1) : 1;
     const int sd = LY::doubles(a.pitch);
 
-    // zero every stage once (the padding of rows shorter than the pitch stays zero)
+    // zero every stage once (rows outside the box and the padding of short rows stay zero)
     for (int i = tid; i < S * sd; i += blockDim.x) smem[i] = 0.0;
     if (tid == 0) {
         for (int s = 0; s < S; ++s) mbar_init(bars + s, 1);
@@ -349,31 +316,16 @@ __device__ __forceinline__ void plane_mv(const CufspPlaneArgs &a, const double *
     fence_proxy_async();
     __syncthreads();
 
-    auto stage_of = [&](int k) { return smem + (k % S) * sd; };
-    auto wait_load = [&](int k) -> bool { return mbar_wait_bounded(bars + k % S, (k / S) & 1, CUFSP_PLANE_WAIT_TRIES); };
-    auto drain_load = [&](int k) -> bool { return mbar_wait_bounded(bars + k % S, (k / S) & 1, 1 << 20); };
-
-    // after a CTA barrier: `count` more stages are free; thread 0 keeps S loads in flight
-    auto refill = [&](int count) {
-        if (tid == 0) {
-            prod.released += count;
-            while (prod.issued - prod.released < S && prod.seg < n_seg) {
-                fence_proxy_async();
-                issue_plane<ACCUM>(a, prod.t, x, y, stage_of(prod.issued), bars + prod.issued % S, prod.p);
-                ++prod.issued;
-                if (++prod.p > prod.t.z1 && ++prod.seg < n_seg) {
-                    prod.t = segment_of(a, prod.seg);
-                    prod.p = prod.t.z0 - 1;
-                }
-            }
-        }
-    };
+    // Planes p >= z0 - 1 map to stage (p - z0 + 1) % S with parity ((p - z0 + 1) / S) & 1.
+    const int pbase = t.z0 - 1;
+    const int p_last = t.z1;  // the halo plane after the segment is the last one read
+    int issued = pbase - 1;
     if (tid == 0) {
-        prod.issued = prod.released = prod.seg = 0;
-        prod.t = segment_of(a, 0);
-        prod.p = prod.t.z0 - 1;
+        const int stop = min(p_last, pbase + S - 1);
+        for (int p = pbase; p <= stop; ++p)
+            issue_plane<ACCUM>(a, t, x, y, smem + ((p - pbase) % S) * sd, bars + (p - pbase) % S, p);
+        issued = stop;
     }
-    refill(0);
 
     // inner factors of the lane's two positions (registers, fixed for the launch)
     double Fa[2][NFA1], Fb[2][NFB1];
@@ -393,36 +345,47 @@ __device__ __forceinline__ void plane_mv(const CufspPlaneArgs &a, const double *
     }
     const double alpha = a.alpha * (a.d_alpha ? __ldg(a.d_alpha) : 1.0);
 
+    auto stage_of = [&](int p) { return smem + ((p - pbase) % S) * sd; };
+    auto wait_plane = [&](int p) -> bool {
+        return mbar_wait_bounded(bars + (p - pbase) % S, ((p - pbase) / S) & 1, CUFSP_PLANE_WAIT_TRIES);
+    };
+    auto drain_plane = [&](int p) -> bool {
+        return mbar_wait_bounded(bars + (p - pbase) % S, ((p - pbase) / S) & 1, 1 << 20);
+    };
+
     bool bad = false;
-    int next = 0;  // the next load to wait for (the loads before it have landed)
-    Slot q0, q1, q2;
-    for (int j = 0; j < n_seg && !bad; ++j) {
-        const Tile t = segment_of(a, j);
-        // prologue: planes z0 - 1 and z0 into the queue; the halo plane's stage is free afterwards
-        const int kbase = next;
-        if (wait_load(kbase) && wait_load(kbase + 1)) {
-            load_slot(L, stage_of(kbase), a.pitch, q2);
-            load_slot(L, stage_of(kbase + 1), a.pitch, q0);
-        } else {
-            failed_flag = 1;
-        }
-        __syncthreads();
-        if (failed_flag) {
-            bad = true;
-            break;
-        }
-        next = kbase + 2;
-        refill(1);
-        // Step z: the slots hold (z - 1, z, z + 1) in a fixed rotation of 3; one barrier per plane.  After
-        // step z the stage of plane z is free (its x rows went into the queue one step earlier, its y rows
-        // and words were used in step z), after the last step also that of the halo plane z1.
-        int z = t.z0;
+    Slot q0, q1, q2, q3;
+    // prologue: planes z0 - 1 and z0 into the queue
+    if (wait_plane(pbase) && wait_plane(t.z0)) {
+        load_slot(L, stage_of(pbase), a.pitch, PPS == 1 ? q2 : q3);
+        load_slot(L, stage_of(t.z0), a.pitch, q0);
+    } else {
+        failed_flag = 1;
+    }
+    __syncthreads();
+    bad = failed_flag != 0;
+    const bool prologue_ok = !bad;
+
+    int z = t.z0;
+    // Refill after a CTA barrier: every stage whose plane the CTA has finished with goes to the next
+    // plane at once -- after the prologue the halo plane z0 - 1, after step z plane z (its x rows went
+    // into the register queue one step earlier, its y rows and words were used in step z).
+    auto refill = [&](int count) {
+        if (tid == 0)
+            for (int k = 0; k < count && issued < p_last; ++k) {
+                ++issued;
+                fence_proxy_async();
+                issue_plane<ACCUM>(a, t, x, y, stage_of(issued), bars + (issued - pbase) % S, issued);
+            }
+    };
+    if (!bad) refill(1);
+    if constexpr (PPS == 1) {
+        // Step z: the slots hold (z - 1, z, z + 1) in a fixed rotation of 3; one barrier per plane.
         auto step = [&](Slot &sm, Slot &s0, Slot &sp) -> bool {
             if (bad || z >= t.z1) return false;
-            const int k = kbase + 1 + (z - t.z0);  // load of plane z
-            if (wait_load(k + 1)) {
-                load_slot(L, stage_of(k + 1), a.pitch, sp);
-                const double *st = stage_of(k);
+            if (wait_plane(z + 1)) {
+                load_slot(L, stage_of(z + 1), a.pitch, sp);
+                const double *st = stage_of(z);
                 compute_rows<ACCUM, 0>(a, L, t, z, sm, s0, sp, st + LY::g_off(a.pitch), st + LY::y_off(a.pitch), Fa,
                                        Fb, alpha, y);
             } else {
@@ -433,18 +396,49 @@ __device__ __forceinline__ void plane_mv(const CufspPlaneArgs &a, const double *
                 bad = true;
                 return false;
             }
-            next = k + 2;
+            refill(1);
             ++z;
-            refill(z == t.z1 ? 2 : 1);
             return true;
         };
         while (step(q2, q0, q1) && step(q0, q1, q2) && step(q1, q2, q0)) {
         }
+    } else {
+        // Double step z: slots (z - 1, z, z + 1, z + 2) in a rotation of 4; planes z and z + 1 are
+        // computed under one barrier (z + 1 only while inside the segment).
+        auto step2 = [&](Slot &sa, Slot &sb, Slot &sc, Slot &sd) -> bool {
+            if (bad || z >= t.z1) return false;
+            const bool two = z + 1 < t.z1;
+            if (wait_plane(z + 1) && (!two || wait_plane(z + 2))) {
+                load_slot(L, stage_of(z + 1), a.pitch, sc);
+                if (two) load_slot(L, stage_of(z + 2), a.pitch, sd);
+                const double *st = stage_of(z);
+                compute_rows<ACCUM, 0>(a, L, t, z, sa, sb, sc, st + LY::g_off(a.pitch), st + LY::y_off(a.pitch), Fa,
+                                       Fb, alpha, y);
+                if (two) {
+                    const double *st1 = stage_of(z + 1);
+                    compute_rows<ACCUM, 0>(a, L, t, z + 1, sb, sc, sd, st1 + LY::g_off(a.pitch),
+                                           st1 + LY::y_off(a.pitch), Fa, Fb, alpha, y);
+                }
+            } else {
+                failed_flag = 1;
+            }
+            __syncthreads();  // the stages of z and z + 1 are consumed
+            if (failed_flag) {
+                bad = true;
+                return false;
+            }
+            refill(two ? 2 : 1);
+            z += two ? 2 : 1;
+            return true;
+        };
+        while (step2(q3, q0, q1, q2) && step2(q1, q2, q3, q0)) {
+        }
     }
     if (tid == 0) {
-        // every issued copy must have landed before the CTA's shared memory is released
-        for (int k = next; k < prod.issued; ++k)
-            if (!drain_load(k)) bad = true;
+        // every issued copy must have landed before the CTA's shared memory is released: after a
+        // failed prologue none was waited for; otherwise the planes up to z were
+        for (int p = prologue_ok ? z + 1 : pbase; p <= issued; ++p)
+            if (!drain_plane(p)) bad = true;
         if (bad) atomicExch(a.err, 1);
     }
 }

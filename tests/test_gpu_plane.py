@@ -182,9 +182,11 @@ def check_general(m, x=None):
 
 @pytest.mark.parametrize("case", ["gene", "odd_states", "big_change", "random5", "toggle_no_plane"])
 def test_specialised_general_kernel_matches_oracle(cuda, case, monkeypatch):
-    """Networks outside the plane kernel's shape use the KRONECKER kernel specialised per network and
-    box (factor kinds ones / identity / table as constants): 5 species, an odd state count, a change
-    of 2 molecules, random 4-species networks, and a plane-shaped network with the plane kernel off."""
+    """The KRONECKER kernel specialised per network and box (factor kinds ones / identity / table as
+    constants; opt-in for the forward action, CUFSP_KRON_RTC=1) on networks outside the plane kernel's
+    shape: 5 species, an odd state count, a change of 2 molecules, random 4-species networks, and a
+    plane-shaped network with the plane kernel off."""
+    monkeypatch.setenv("CUFSP_KRON_RTC", "1")
     if case == "gene":
         m = models.gene_expression((1, 1, 1, 63, 40), time_varying=False)
     elif case == "odd_states":
@@ -204,10 +206,12 @@ def test_specialised_general_kernel_matches_oracle(cuda, case, monkeypatch):
 
 
 def test_generic_kernel_remains(cuda, monkeypatch):
-    """With the specialised kernels switched off the generic k_kron_mv serves the generator, to the
-    same bar."""
-    monkeypatch.setenv("CUFSP_KRON_RTC", "0")
+    """By default (and with the specialised kernels switched off) the generic k_kron_mv serves the
+    forward action of networks outside the plane kernel's shape, to the same bar."""
     monkeypatch.setenv("CUFSP_PLANE", "0")
+    A = check_general(models.gene_expression((1, 1, 1, 20, 11), time_varying=False))
+    assert "k_kron_mv" in A.describe(), A.describe()
+    monkeypatch.setenv("CUFSP_KRON_RTC", "0")
     for m in (models.gene_expression((1, 1, 1, 40, 23), time_varying=False), models.mass_action_3(bounds=(20, 9, 9))):
         A = check_general(m)
         assert "k_kron_mv" in A.describe(), A.describe()
