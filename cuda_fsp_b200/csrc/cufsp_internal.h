@@ -170,7 +170,8 @@ bool plane_launch(PlaneData *pd, const double *coefs, double alpha, const double
                   cufsp_status *status);
 // Coefficient-dependent tables of the plane kernel (row words), rebuilt when the coefficients change.
 cufsp_status plane_prepare(PlaneData *pd, const double *coefs, cudaStream_t st);
-cufsp_status kron_prepare(KronData *k, const double *coefs, cudaStream_t st);
+// transpose: the transposed action will follow (its kernel is compiled here, outside any capture).
+cufsp_status kron_prepare(KronData *k, const double *coefs, cudaStream_t st, bool transpose = false);
 // Human-readable kernel choice of a KRONECKER generator.
 std::string kron_describe(const KronData *k);
 
@@ -217,7 +218,7 @@ cufsp_status mat_coefs(cufsp_mat *A, double t, const double *coefs_in, std::vect
 cufsp_status mat_check_watchdog(cufsp_mat *A, const char *where);
 // Bring the generator's coefficient-dependent device tables up to `coefs` (stream order); applies
 // captured in a CUDA graph after this call launch nothing else.
-cufsp_status mat_prepare(cufsp_mat *A, const double *coefs, cudaStream_t st);
+cufsp_status mat_prepare(cufsp_mat *A, const double *coefs, cudaStream_t st, bool transpose = false);
 // y = alpha * A(coefs)^T x (overwrite); KRONECKER generators only.
 cufsp_status mat_apply_transpose(cufsp_mat *A, const double *coefs, double alpha, const double *d_alpha,
                                  const int *d_skip, const double *x, double *y, cudaStream_t st);

@@ -786,7 +786,23 @@ int kron_watchdog(KronData *k) {
 int64_t kron_halo(const KronData *k) { return k->plane ? std::max<int64_t>(k->halo, plane_size(k->plane)) : k->halo; }
 int64_t kron_row_len(const KronData *k) { return k->plane ? plane_size(k->plane) : k->L; }
 
-cufsp_status kron_prepare(KronData *k, const double *coefs, cudaStream_t st) {
+namespace {
+// The specialised kernel is compiled (NVRTC) and its tables copied at its first use -- never while
+// `st` is being captured into a graph, where those calls are not allowed: drivers that capture call
+// kron_prepare first, and an apply met during a capture falls back to the generic kernels.
+void ensure_rtc(KronData *k, cudaStream_t st) {
+    if (k->rtc_tried || !k->model) return;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    if (cs == cudaStreamCaptureStatusNone) kron_build_rtc(*k->model, k);
+}
+}  // namespace
+
+cufsp_status kron_prepare(KronData *k, const double *coefs, cudaStream_t st, bool transpose) {
+    if (transpose || k->rtc_forward) ensure_rtc(k, st);
     return k->plane ? plane_prepare(k->plane, coefs, st) : CUFSP_SUCCESS;
 }
 
@@ -850,7 +866,7 @@ __global__ void __launch_bounds__(256) k_kron_mvT(const KronTArgs a, const doubl
 
 cufsp_status kron_apply_transpose(KronData *kd, const double *coefs, double alpha, const double *d_alpha,
                                   const int *d_skip, const double *x, double *y, cudaStream_t st) {
-    if (!kd->rtc_tried && kd->model) kron_build_rtc(*kd->model, kd);
+    ensure_rtc(kd, st);
     if (kd->rtc && ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) % 16) == 0) {
         CufspKronRtcArgs r;
         std::memset(&r, 0, sizeof(r));
@@ -913,7 +929,7 @@ cufsp_status kron_apply(KronData *kd, const double *coefs, double alpha, const d
             return CUFSP_SUCCESS;
         }
     }
-    if (kd->rtc_forward && !kd->rtc_tried && kd->model) kron_build_rtc(*kd->model, kd);
+    if (kd->rtc_forward) ensure_rtc(kd, st);
     if (kd->rtc_forward && kd->rtc &&
         ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) % 16) == 0) {
         if (i_end < 0) i_end = kd->n;

@@ -317,7 +317,7 @@ cufsp_status arnoldi_pass(cufsp_expv *E, double *v, cudaStream_t st, bool with_a
     } else if (E->A && graphs_enabled()) {
         *E->h_btol = btol_eff;  // the previous pass's copy has completed: the stream was synchronised after it
         CUFSP_CUDA_TRY(cudaMemcpyAsync(E->ks.btol, E->h_btol, sizeof(double), cudaMemcpyHostToDevice, st));
-        s = mat_prepare(E->A, E->coefs.data(), st);
+        s = mat_prepare(E->A, E->coefs.data(), st, E->transpose);
         if (s != CUFSP_SUCCESS) return s;
         cudaGraphExec_t exec = nullptr;
         for (auto &g : E->graphs)

@@ -29,8 +29,8 @@ cufsp_status mat_apply(cufsp_mat *A, const double *coefs, double alpha, const do
     return sparse_apply(A->sparse, coefs, alpha, d_alpha, d_skip, x, accumulate, y, st, i_begin, i_end);
 }
 
-cufsp_status mat_prepare(cufsp_mat *A, const double *coefs, cudaStream_t st) {
-    return A->kron ? kron_prepare(A->kron, coefs, st) : CUFSP_SUCCESS;
+cufsp_status mat_prepare(cufsp_mat *A, const double *coefs, cudaStream_t st, bool transpose) {
+    return A->kron ? kron_prepare(A->kron, coefs, st, transpose) : CUFSP_SUCCESS;
 }
 
 cufsp_status mat_apply_transpose(cufsp_mat *A, const double *coefs, double alpha, const double *d_alpha,
