@@ -681,7 +681,10 @@ def run_leg(args):
       adjoint one log-likelihood gradient on the gene model (--box, default 1,1,1,127,127)
       gradbatch  gradients of --sets parameter sets with --workers concurrent host workers
       bdf     the BDF solve of the time-varying gene model to t = 6 (--box)
-      states  state enumeration cufsp_get_states (--box, default 1023,1023,3)"""
+      states  state enumeration cufsp_get_states (--box, default 1023,1023,3)
+      iopsweep  exp(tA)p0 on mass_action_3 (--box, default 255^3) to t = 0.2 for Krylov dimensions m and
+              incomplete orthogonalisation depths q, each timed to completion, with its 1-norm distance
+              to an m = 60, tol 1e-11 full-orthogonalisation solution"""
     import torch
     from cuda_fsp_b200 import (BDFIntegrator, FSPMat, KryExpvFSP, Likelihood, MatrixFormat, get_states, models)
     box = [int(v) for v in args.box.split(",")] if args.box else None
@@ -778,6 +781,35 @@ def run_leg(args):
         B.advance(6.0, p)
         torch.cuda.synchronize()
         out.update({"n_states": m.n_states, "s_to_t6": round(time.perf_counter() - t0, 4), "steps": B.stats["n_steps"]})
+    elif args.leg == "iopsweep":
+        m = models.mass_action_3(bounds=box) if box else models.mass_action_3()
+        A = FSPMat.from_model(m, MatrixFormat.KRONECKER)
+        p0 = torch.as_tensor(m.p0(), device="cuda")
+        T = 0.2
+
+        def solve(tol, **kw):
+            v = p0.clone()
+            KryExpvFSP(T, A, v, tol=tol, coefs=m.coefs(0), **kw).step()  # warm-up: tables, first launches
+            v.copy_(p0)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            E = KryExpvFSP(T, A, v, tol=tol, coefs=m.coefs(0), **kw)
+            E.max_nstep = 1 << 20
+            st = E.solve()
+            torch.cuda.synchronize()
+            return v, time.perf_counter() - t0, st
+
+        ref, dt_ref, st_ref = solve(1e-11, m=60)
+        rows = []
+        for mk, q in ((30, 0), (45, 0), (60, 0), (30, 2), (45, 2), (60, 2), (60, 3), (60, 4)):
+            kw = dict(m=mk, iop=q > 0, q_iop=max(q, 1))
+            v, dt, st = solve(1e-8, **kw)
+            rows.append({"m": mk, "q": q or "full", "s": round(dt, 3), "steps": st["n_steps"],
+                         "rejected": st["n_reject"], "matvecs": st["n_matvec"],
+                         "err_1norm": float((v - ref).abs().sum().item())})
+        out.update({"n_states": m.n_states, "t": T, "tol": 1e-8,
+                    "reference": {"m": 60, "tol": 1e-11, "s": round(dt_ref, 3), "steps": st_ref["n_steps"]},
+                    "configs": rows})
     elif args.leg == "states":
         b = box or [1023, 1023, 3]
         st = get_states(b)
@@ -802,7 +834,8 @@ def main():
     ap.add_argument("--sets", type=int, default=4, help="rotating (x, y) input pairs; parameter sets of the gradbatch leg")
     ap.add_argument("--no-extras", action="store_true",
                     help="time the generator action only (no e2e, expmv or CPU legs); for profiling runs")
-    ap.add_argument("--leg", choices=["sparse", "kgen", "krylov", "adjoint", "gradbatch", "bdf", "states"], default=None,
+    ap.add_argument("--leg", choices=["sparse", "kgen", "krylov", "adjoint", "gradbatch", "bdf", "states", "iopsweep"],
+                    default=None,
                     help="run one leg alone (profiling runs; see run_leg)")
     ap.add_argument("--box", default=None, help="box bounds of the leg, comma separated")
     ap.add_argument("--workers", type=int, default=2, help="host workers of the gradbatch leg")

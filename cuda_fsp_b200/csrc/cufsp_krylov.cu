@@ -66,6 +66,8 @@ __global__ void __launch_bounds__(kRedThreads) k_step_begin(int64_t n, const dou
 
 struct MVecArgs {
     const double *vec[kMaxVec];
+    const double *v0;  // W_0 (the caller's vector)
+    const double *W;   // W_1 .. W_{m+1}, contiguous with stride n
     double *w;
     int64_t n;
     int K;      // number of basis vectors used (istart..j)
@@ -99,6 +101,89 @@ __global__ void __launch_bounds__(kRedThreads) k_mdot(const MVecArgs a) {
         a.s.H[kk + a.j * a.s.mp2] = h;
         a.s.gam[kk] = h * r;
     }
+}
+
+// Same result with the vectors split over groups of warps: warp w of a CTA serves the vector group
+// g = w % G (vectors g*Kb .. g*Kb + Kg - 1, Kb = ceil(K / G) <= KG) over the states of slice w / G of
+// the CTA's tile.  Each thread keeps KG sums instead of K, so the CTA stays at high occupancy for
+// K up to 64 and every element of w is fetched from DRAM once per CTA (the G warps of a slice share
+// it through L1).  With TWO, each lane takes two states 32 apart per tile, so that twice as many
+// loads are in flight per thread (3 CTAs per SM instead of 4).
+template <int KG, int G, bool TWO>
+__global__ void __launch_bounds__(kRedThreads, TWO ? 3 : 4) k_mdot_grouped(const MVecArgs a) {
+    constexpr int KP = KG * G;
+    constexpr int S = kRedWarps / G;  // state slices of 32 (64 with TWO) in a CTA tile
+    constexpr int L = TWO ? 64 : 32;
+    static_assert(S * G == kRedWarps, "G must divide the warps of a CTA");
+    __shared__ RedSmem<KP> sm;
+    if (*a.s.flag) return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = warp % G, slice = warp / G;
+    const int Kb = (a.K + G - 1) / G;
+    const int k0 = g * Kb;
+    const int Kg = max(0, min(Kb, a.K - k0));
+    // Basis vector kbase + k0 + kk: W_0 is the caller's vector, W_1.. are contiguous (stride n).
+    const int ka = a.kbase + k0;
+    const double *p_first = ka == 0 ? a.v0 : a.W + (int64_t)(ka - 1) * a.n;
+    const double *p_next = a.W + (int64_t)ka * a.n;  // vector ka + 1; read only when Kg > 1
+    double acc[KG];
+#pragma unroll
+    for (int kk = 0; kk < KG; ++kk) acc[kk] = 0.0;
+    constexpr int64_t tile = (int64_t)S * L;
+    const int64_t stride = (int64_t)gridDim.x * tile;
+    for (int64_t i0 = (int64_t)blockIdx.x * tile + slice * L + lane; i0 < a.n; i0 += stride) {
+        const int64_t i1 = i0 + 32;
+        const bool two = TWO && i1 < a.n;
+        const double w0 = __ldg(a.w + i0);
+        const double w1 = two ? __ldg(a.w + i1) : 0.0;
+        double u0[KG], u1[KG];
+        if (Kg > 0) {
+            u0[0] = __ldg(p_first + i0);
+            u1[0] = two ? __ldg(p_first + i1) : 0.0;
+        }
+        const double *q = p_next + i0;
+#pragma unroll
+        for (int kk = 1; kk < KG; ++kk) {
+            if (kk < Kg) {
+                u0[kk] = __ldg(q);
+                u1[kk] = two ? __ldg(q + 32) : 0.0;
+                q += a.n;
+            }
+        }
+#pragma unroll
+        for (int kk = 0; kk < KG; ++kk)
+            if (kk < Kg) acc[kk] = TWO ? fma(u1[kk], w1, fma(u0[kk], w0, acc[kk])) : fma(u0[kk], w0, acc[kk]);
+    }
+#pragma unroll
+    for (int kk = 0; kk < KG; ++kk) {
+        if (kk < Kg) {
+            double v = acc[kk];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0) sm.warp_part[warp][kk] = v;
+        }
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < a.K; k += blockDim.x) {
+        const int gg = k / Kb, kk = k - gg * Kb;
+        double v = 0.0;
+        for (int s = 0; s < S; ++s) v += sm.warp_part[s * G + gg][kk];
+        a.partials[(size_t)blockIdx.x * KP + k] = v;
+    }
+    if (!grid_finish<KP>(a.K, a.partials, a.counter, sm)) return;
+    for (int k = threadIdx.x; k < a.K; k += blockDim.x) {
+        const int kk = a.kbase + k;
+        const double r = a.s.rho[kk];
+        const double h = r * sm.final_[k];
+        a.s.H[kk + a.j * a.s.mp2] = h;
+        a.s.gam[kk] = h * r;
+    }
+}
+
+template <int KG, int G>
+void launch_mdot_grouped(const MVecArgs &a, int mode, int sm_count, cudaStream_t st) {
+    if (mode == 2) k_mdot_grouped<KG, G, true><<<3 * sm_count, kRedThreads, 0, st>>>(a);
+    else k_mdot_grouped<KG, G, false><<<4 * sm_count, kRedThreads, 0, st>>>(a);
 }
 
 // W_{j+1} -= sum_k gam_k W_k;  s = rho_j-scaled norm;  H(j+1, j) = s;  rho_{j+1} = 1/s;
@@ -231,6 +316,17 @@ cufsp_status matvec(cufsp_expv *E, const double *x, double *y, const double *d_a
     return launch_scale(E->n, y, d_alpha, 1.0, st);
 }
 
+// Multi-vector dot kernel: CUFSP_KRYLOV_MDOT=0 one thread over all vectors (k_mdot), 1 vectors split
+// over warp groups (k_mdot_grouped), 2 the same with two states per lane (default).
+int mdot_mode() {
+    static const int mode = [] {
+        const char *e = getenv("CUFSP_KRYLOV_MDOT");
+        const int v = e ? atoi(e) : 2;
+        return v < 0 || v > 2 ? 2 : v;
+    }();
+    return mode;
+}
+
 template <int KP>
 void launch_mdot(const MVecArgs &a, int grid, cudaStream_t st) { k_mdot<KP><<<grid, kRedThreads, 0, st>>>(a); }
 template <int KP>
@@ -243,6 +339,8 @@ cufsp_status arnoldi_dot_update(cufsp_expv *E, double *v, int j, int istart, cud
     a.K = j - istart + 1;
     a.kbase = istart;
     for (int k = 0; k < a.K; ++k) a.vec[k] = wvec(E, v, istart + k);
+    a.v0 = v;
+    a.W = E->W;
     a.w = wvec(E, v, j + 1);
     a.n = E->n;
     a.j = j;
@@ -250,10 +348,22 @@ cufsp_status arnoldi_dot_update(cufsp_expv *E, double *v, int j, int istart, cud
     a.partials = E->rs.partials;
     a.counter = E->rs.counter;
     const int K = a.K;
-    if (K <= 8) launch_mdot<8>(a, E->grid, st);
-    else if (K <= 16) launch_mdot<16>(a, E->grid, st);
-    else if (K <= 32) launch_mdot<32>(a, E->grid, st);
-    else launch_mdot<64>(a, E->grid, st);
+    const int mode = mdot_mode();
+    const int sms = device_info().sm_count;
+    if (mode == 0 || E->grid < 4 * sms) {  // small vectors: the grid of the other pass kernels
+        if (K <= 8) launch_mdot<8>(a, E->grid, st);
+        else if (K <= 16) launch_mdot<16>(a, E->grid, st);
+        else if (K <= 32) launch_mdot<32>(a, E->grid, st);
+        else launch_mdot<64>(a, E->grid, st);
+    } else if (K <= 8) {
+        launch_mdot_grouped<8, 1>(a, mode, sms, st);
+    } else if (K <= 16) {
+        launch_mdot_grouped<8, 2>(a, mode, sms, st);
+    } else if (K <= 32) {
+        launch_mdot_grouped<8, 4>(a, mode, sms, st);
+    } else {
+        launch_mdot_grouped<8, 8>(a, mode, sms, st);
+    }
     CUFSP_CUDA_TRY(cudaGetLastError());
     if (K <= 8) launch_mupd<8>(a, E->grid, st);
     else if (K <= 16) launch_mupd<16>(a, E->grid, st);

@@ -20,27 +20,12 @@ struct RedSmem {
     int is_last;
 };
 
-// acc[0..K-1] hold this thread's partial sums (K <= KP).  On return, `true` in every thread of
-// the last CTA, with the grid totals in sm.final_[0..K-1] (visible after the call).
+// Second half of a grid reduction: this CTA's totals for outputs 0..K-1 are already in
+// partials[blockIdx.x * KP + k].  Returns `true` in every thread of the last CTA to arrive, with the
+// grid totals in sm.final_[0..K-1] (visible after the call); sm.warp_part is reused as scratch.
 template <int KP>
-__device__ __forceinline__ bool grid_reduce(double (&acc)[KP], int K, double *__restrict__ partials,
-                                            unsigned int *__restrict__ counter, RedSmem<KP> &sm) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-    for (int k = 0; k < KP; ++k) {
-        if (k < K) {
-            double v = acc[k];
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            if (lane == 0) sm.warp_part[warp][k] = v;
-        }
-    }
-    __syncthreads();
-    for (int k = threadIdx.x; k < K; k += blockDim.x) {
-        double v = 0.0;
-        for (int w = 0; w < kRedWarps; ++w) v += sm.warp_part[w][k];
-        partials[(size_t)blockIdx.x * KP + k] = v;
-    }
+__device__ __forceinline__ bool grid_finish(int K, double *__restrict__ partials, unsigned int *__restrict__ counter,
+                                            RedSmem<KP> &sm) {
     __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -74,6 +59,30 @@ __device__ __forceinline__ bool grid_reduce(double (&acc)[KP], int K, double *__
     if (threadIdx.x == 0) *counter = 0u;  // ready for the next launch on this stream
     __syncthreads();
     return true;
+}
+
+// acc[0..K-1] hold this thread's partial sums (K <= KP).  On return, `true` in every thread of
+// the last CTA, with the grid totals in sm.final_[0..K-1] (visible after the call).
+template <int KP>
+__device__ __forceinline__ bool grid_reduce(double (&acc)[KP], int K, double *__restrict__ partials,
+                                            unsigned int *__restrict__ counter, RedSmem<KP> &sm) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < KP; ++k) {
+        if (k < K) {
+            double v = acc[k];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0) sm.warp_part[warp][k] = v;
+        }
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < K; k += blockDim.x) {
+        double v = 0.0;
+        for (int w = 0; w < kRedWarps; ++w) v += sm.warp_part[w][k];
+        partials[(size_t)blockIdx.x * KP + k] = v;
+    }
+    return grid_finish<KP>(K, partials, counter, sm);
 }
 
 }  // namespace cufsp
