@@ -123,6 +123,7 @@ SIGNATURES = {
     "cufsp_mat_dims": [_P, _IP, _IP, _IP],
     "cufsp_mat_action": [_P, C.c_double, _P, _P, _P],
     "cufsp_mat_apply": [_P, C.c_double, _DP, C.c_double, _P, C.c_double, _P, _P],
+    "cufsp_mat_apply_transpose": [_P, C.c_double, _DP, C.c_double, _P, _P, _P],
     "cufsp_mat_action_host": [_P, C.c_double, _P, _P],
     "cufsp_mat_export_propensities": [_P, _P, _P],
     "cufsp_mat_watchdog": [_P, _IP],

@@ -25,6 +25,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <numeric>
 
 #include <sstream>
 
@@ -322,6 +323,12 @@ struct KronData {
     std::string rtc_why;
     bool rtc_tried = false;       // built at the first transposed action (or at create when it serves the forward)
     bool rtc_forward = false;     // CUFSP_KRON_RTC=1: it also serves the forward action
+    // row kernels of the same module (cufsp_kron_rows_*): inner factors fixed per lane
+    bool rows_forward = false;    // they serve the forward action
+    bool rows_transpose = false;  // and the transposed one
+    int rows_k = 1;               // inner species
+    int64_t rows_L = 1;           // inner positions per row
+    int rows_grid = 0;
     const ModelHost *model = nullptr;  // the generator's model (outlives this object), for the lazy build
 };
 
@@ -521,11 +528,46 @@ static void kron_build_rtc(const ModelHost &m, KronData *kd) {
     const int chunk = std::max(1, std::min(nr, env_or("CUFSP_KRON_RTC_CHUNK", 5)));
     const int minb = std::max(1, std::min(8, env_or("CUFSP_KRON_RTC_MINB", 2)));
     const bool tab_smem = packed.size() * sizeof(double) <= 40960;
+    // Row kernels: the inner species are the leading ones up to the last, while a row stays within
+    // 65,536 positions.
+    int rk = 1;
+    int64_t rL = (int64_t)m.bounds[0] + 1;
+    while (rk + 1 < ns && rL * ((int64_t)m.bounds[rk] + 1) <= 65536) rL *= (int64_t)m.bounds[rk++] + 1;
+    // Terms as the kernel forms them: reactions with one shift whose outer factors are all ones share
+    // a gather.  Positions per lane from the per-lane register need (terms x positions): 4 up to 12
+    // terms (one 8-warp CTA per SM, 40+ loads in flight per lane: 3.25 TB/s on the 12-reaction gene
+    // network at 8.4M states, against 2.88 at 2 positions and 2 CTAs/SM, 2.43 at 1 and 3 CTAs/SM).
+    int n_terms = 0;
+    {
+        std::vector<int64_t> merged;
+        for (int r = 0; r < nr; ++r) {
+            bool outer_one = true;
+            for (int s2 = rk; s2 < ns; ++s2)
+                if (m.nu[(size_t)r * ns + s2] != 0 || kind[(size_t)r * ns + s2] != 0) outer_one = false;
+            int64_t d = 0;
+            for (int s2 = 0; s2 < ns; ++s2) d += (int64_t)m.nu[(size_t)r * ns + s2] * stride[s2];
+            if (!outer_one) {
+                ++n_terms;
+            } else if (std::find(merged.begin(), merged.end(), d) == merged.end()) {
+                merged.push_back(d);
+                ++n_terms;
+            }
+        }
+    }
+    int rv = env_or("CUFSP_KRON_ROWS_V", n_terms <= 12 ? 4 : (n_terms <= 24 ? 2 : 1));
+    rv = rv >= 4 ? 4 : (rv == 2 ? 2 : 1);
+    while (rv > 1 && 32LL * rv > rL) rv /= 2;  // short rows: no idle lanes
+    const int rchunk = std::max(1, std::min(nr, env_or("CUFSP_KRON_ROWS_CHUNK", 12)));
+    const int rminb = std::max(1, std::min(8, env_or("CUFSP_KRON_ROWS_MINB", rv == 4 ? 1 : (rv == 2 ? 2 : 3))));
+    kd->rows_k = rk;
+    kd->rows_L = rL;
     std::ostringstream o;
     o << "#define CUFSP_KRON_MINB " << minb << "\n#define CUFSP_KRON_RTC_MAX_R " << CUFSP_KRON_RTC_MAX_R
       << "\n#define CUFSP_KRON_NS " << ns << "\n#define CUFSP_KRON_NR " << nr << "\n#define CUFSP_KRON_N " << m.n
       << "LL\n#define CUFSP_KRON_CHUNK " << chunk << "\n#define CUFSP_KRON_TS " << std::max<size_t>(1, packed.size())
-      << "\n#define CUFSP_KRON_TAB_SMEM " << (tab_smem ? 1 : 0) << "\nnamespace cufsp_kron {\n";
+      << "\n#define CUFSP_KRON_TAB_SMEM " << (tab_smem ? 1 : 0) << "\n#define CUFSP_KRON_K " << rk
+      << "\n#define CUFSP_KRON_V " << rv << "\n#define CUFSP_KRON_L " << rL << "LL\n#define CUFSP_KRON_RCHUNK " << rchunk
+      << "\n#define CUFSP_KRON_ROWS_MINB " << rminb << "\nnamespace cufsp_kron {\n";
     o << "__device__ __forceinline__ constexpr int ext(int s) {";
     for (int s = 0; s < ns; ++s) o << " if (s == " << s << ") return " << m.bounds[s] + 1 << ";";
     o << " return 1; }\n";
@@ -548,7 +590,9 @@ static void kron_build_rtc(const ModelHost &m, KronData *kd) {
     }
     o << " return 0; }\n}\n";
     std::string why;
-    auto mod = rtc_module(o.str() + kKronRtcSource, {"cufsp_kron_mv_accum", "cufsp_kron_mv_set", "cufsp_kron_mvT_set"},
+    auto mod = rtc_module(o.str() + kKronRtcSource,
+                          {"cufsp_kron_mv_accum", "cufsp_kron_mv_set", "cufsp_kron_mvT_set", "cufsp_kron_rows_accum",
+                           "cufsp_kron_rows_set", "cufsp_kron_rowsT_set"},
                           why);
     if (!mod) {
         kd->rtc_why = why;
@@ -570,6 +614,19 @@ static void kron_build_rtc(const ModelHost &m, KronData *kd) {
     }
     kd->rtc = mod;
     kd->rtc_grid = device_info().sm_count * occ;
+    // Row kernels: a persistent grid whose warp count is a multiple of the chunks per row, so that
+    // each warp keeps one chunk (and computes its inner factors once).
+    int rocc = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&rocc, (const void *)mod->kernels[3], 256, 0) != cudaSuccess ||
+        rocc < 1) {
+        cudaGetLastError();
+        kd->rows_forward = kd->rows_transpose = false;
+        return;
+    }
+    const int64_t nch = (rL + 32LL * rv - 1) / (32LL * rv);
+    const int64_t resident = (int64_t)device_info().sm_count * rocc;
+    const int64_t h = nch / std::gcd<int64_t>(nch, 8);  // CTAs per group of 8h warps = h chunks x 8 rows
+    kd->rows_grid = (int)(h <= resident ? (resident / h) * h : resident);
 }
 
 template <int NR, int V>
@@ -750,7 +807,12 @@ cufsp_status kron_create(const ModelHost &m, KronData **out) {
     // state, which on the 12-reaction gene network at 8.4M states is issue-bound (1.76 TB/s) where the
     // generic kernel, sharing inner and outer factor products across a row, moves 1.92 TB/s.
     kd->rtc_forward = env_or("CUFSP_KRON_RTC", -1) == 1;
-    if (kd->rtc_forward && !kd->plane) kron_build_rtc(m, kd);
+    // Row kernels for the networks the plane kernel does not take (CUFSP_KRON_ROWS=0: off, 1: also
+    // below 65,536 states, where the generic kernel is the default to spare small models a compile).
+    const int rows_env = env_or("CUFSP_KRON_ROWS", -1);
+    kd->rows_forward = !kd->plane && rows_env != 0 && (rows_env == 1 || m.n >= 65536);
+    kd->rows_transpose = rows_env != 0 && (rows_env == 1 || m.n >= 65536);
+    if ((kd->rtc_forward || kd->rows_forward) && !kd->plane) kron_build_rtc(m, kd);
     plan_march(m, kd);
     if (kd->march && kd->ma.k != kd->k) {  // the marching split needs its own outer table
         const std::vector<double2> gm = outer_table(m, kd, kd->ma.k);
@@ -802,12 +864,16 @@ void ensure_rtc(KronData *k, cudaStream_t st) {
 }  // namespace
 
 cufsp_status kron_prepare(KronData *k, const double *coefs, cudaStream_t st, bool transpose) {
-    if (transpose || k->rtc_forward) ensure_rtc(k, st);
+    if (transpose || k->rtc_forward || k->rows_forward) ensure_rtc(k, st);
     return k->plane ? plane_prepare(k->plane, coefs, st) : CUFSP_SUCCESS;
 }
 
 std::string kron_describe(const KronData *k) {
     if (k->plane) return plane_description(k->plane);
+    if (k->rows_forward && k->rtc && k->rows_grid > 0)
+        return "row kernel specialised for the network and box (NVRTC, sm_100a): " + std::to_string(k->rows_k) +
+               " inner species, rows of " + std::to_string(k->rows_L) + " positions, " + std::to_string(k->rows_grid) +
+               " CTAs x 256 threads; plane kernel not used: " + k->plane_why;
     if (k->rtc_forward && k->rtc)
         return "kernel specialised for the network and box (NVRTC, sm_100a), " + std::to_string(k->rtc_grid) +
                " CTAs x 256 threads; plane kernel not used: " + k->plane_why;
@@ -864,9 +930,28 @@ __global__ void __launch_bounds__(256) k_kron_mvT(const KronTArgs a, const doubl
     }
 }
 
+// One launch of a row kernel (module kernel index `which`: 3 accumulate, 4 overwrite, 5 transposed) over
+// all rows.  Plain 8-byte loads and stores: no alignment requirement on x and y.
+static cufsp_status rows_launch(KronData *kd, const double *coefs, double alpha, const double *d_alpha,
+                                const int *d_skip, const double *x, double *y, int which, cudaStream_t st) {
+    CufspKronRtcArgs r;
+    std::memset(&r, 0, sizeof(r));
+    r.tables = kd->d_rtc_tab;
+    r.d_alpha = d_alpha;
+    r.d_skip = d_skip;
+    r.q_begin = 0;
+    r.q_end = kd->n / kd->rows_L;
+    for (int k = 0; k < kd->nr; ++k) r.coef[k] = alpha * coefs[k];
+    void *args[] = {&r, (void *)&x, (void *)&y};
+    CUFSP_CUDA_TRY(cudaLaunchKernel((const void *)kd->rtc->kernels[which], dim3(kd->rows_grid), dim3(256), args, 0, st));
+    return CUFSP_SUCCESS;
+}
+
 cufsp_status kron_apply_transpose(KronData *kd, const double *coefs, double alpha, const double *d_alpha,
                                   const int *d_skip, const double *x, double *y, cudaStream_t st) {
     ensure_rtc(kd, st);
+    if (kd->rows_transpose && kd->rtc && kd->rows_grid > 0)
+        return rows_launch(kd, coefs, alpha, d_alpha, d_skip, x, y, 5, st);
     if (kd->rtc && ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) % 16) == 0) {
         CufspKronRtcArgs r;
         std::memset(&r, 0, sizeof(r));
@@ -928,6 +1013,10 @@ cufsp_status kron_apply(KronData *kd, const double *coefs, double alpha, const d
             CUFSP_CUDA_TRY(cudaGetLastError());
             return CUFSP_SUCCESS;
         }
+    }
+    if (kd->rows_forward && full) {
+        ensure_rtc(kd, st);
+        if (kd->rtc && kd->rows_grid > 0) return rows_launch(kd, coefs, alpha, d_alpha, d_skip, x, y, accumulate ? 3 : 4, st);
     }
     if (kd->rtc_forward) ensure_rtc(kd, st);
     if (kd->rtc_forward && kd->rtc &&

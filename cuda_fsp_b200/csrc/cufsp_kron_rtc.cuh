@@ -25,6 +25,7 @@ struct CufspKronRtcArgs {
     const double *d_alpha;  // nullable device scalar multiplying every coefficient
     const int *d_skip;      // nullable: return at once when *d_skip != 0
     long long i_begin, i_end;
+    long long q_begin, q_end;  // row range of the row kernels (cufsp_kron_rows_*)
     double coef[CUFSP_KRON_RTC_MAX_R];  // alpha * c_r
 };
 
@@ -241,6 +242,301 @@ extern "C" __global__ void __launch_bounds__(256, CUFSP_KRON_MINB) cufsp_kron_mv
                                                                                      const double *__restrict__ x,
                                                                                      double *__restrict__ y) {
     cufsp_kron::kron_mv<false, true>(a, x, y);
+}
+
+// ---- Row kernels: inner factors fixed per lane ------------------------------------------------
+// The state index is split i = q * LEN + p: p covers the inner species 0 .. KI-1 (LEN positions), the
+// row q the outer species KI .. NS-1.  A warp owns VP * 32 positions of one row chunk, lane-contiguous
+// (p = chunk * 32 VP + v * 32 + lane), and sweeps the rows of its chunk; every gather x[i - d_r] is
+// then one 256-byte warp access.  The inner factor products of a lane's positions, already multiplied
+// by alpha * c_r, are computed once per chunk into registers:
+//   A_r(p) = alpha c_r prod_{s<KI} f_{r,s}(p_s - nu_{r,s}) 1{inner source in box}
+//   D0(p)  = sum over reactions whose outer factors are all ones of alpha c_r prod_{s<KI} f_{r,s}(p_s)
+//   E_r(p) = alpha c_r prod_{s<KI} f_{r,s}(p_s) for the other reactions,
+// and the outer factors once per row: G_r(q) (source, 0 outside the box) and Gd_r(q) (state), both
+// the constant 1 -- folded away at compile time -- for reactions that leave the outer species alone.
+// Per state and reaction the work is one gather and one or two FP64 operations:
+//   y[i] (+)= sum_r A_r(p) G_r(q) x[i - d_r] - x[i] (D0(p) + sum_r E_r(p) Gd_r(q)).
+// The transposed action takes A_r = alpha c_r prod_{s<KI} f_{r,s}(p_s) 1{inner target in box},
+// G_r = prod_{s>=KI} f_{r,s}(q_s) 1{outer target in box} and the gather at x[i + d_r].
+
+namespace cufsp_kron {
+
+constexpr int KI = CUFSP_KRON_K;
+constexpr int VP = CUFSP_KRON_V;
+constexpr long long LEN = CUFSP_KRON_L;
+constexpr long long NCH = (LEN + 32 * VP - 1) / (32 * VP);
+constexpr int RC = CUFSP_KRON_RCHUNK;
+constexpr int NO = NS - KI > 0 ? NS - KI : 1;  // outer species (array extent)
+
+__device__ __forceinline__ constexpr bool outer_src_one(int r) {
+    for (int s = KI; s < NS; ++s)
+        if (nu(r, s) != 0 || kind(r, s) != 0) return false;
+    return true;
+}
+__device__ __forceinline__ constexpr bool outer_diag_one(int r) {
+    for (int s = KI; s < NS; ++s)
+        if (kind(r, s) != 0) return false;
+    return true;
+}
+// Terms: reactions with the same shift whose outer factors are all ones share one gather and one
+// per-lane factor (their A_r summed); every other reaction is a term of its own.
+__device__ __forceinline__ constexpr int term_owner(int r) {  // first reaction of r's term
+    if (!outer_src_one(r)) return r;
+    for (int u = 0; u < r; ++u)
+        if (outer_src_one(u) && shift(u) == shift(r)) return u;
+    return r;
+}
+__device__ __forceinline__ constexpr int term_of(int r) {  // owners before r's owner
+    int t = 0;
+    for (int u = 0; u < term_owner(r); ++u) t += term_owner(u) == u ? 1 : 0;
+    return t;
+}
+__device__ __forceinline__ constexpr int n_terms() {
+    int t = 0;
+    for (int u = 0; u < NR; ++u) t += term_owner(u) == u ? 1 : 0;
+    return t;
+}
+__device__ __forceinline__ constexpr int term_rep(int t) {  // owner reaction of term t
+    for (int u = 0; u < NR; ++u)
+        if (term_owner(u) == u && term_of(u) == t) return u;
+    return 0;
+}
+constexpr int NT = n_terms();
+
+// Largest and smallest shift d_r (gathers at i - d_r; the transposed pass negates them).
+__device__ __forceinline__ constexpr long long shift_max() {
+    long long m = 0;
+    for (int r = 0; r < NR; ++r) m = shift(r) > m ? shift(r) : m;
+    return m;
+}
+__device__ __forceinline__ constexpr long long shift_min() {
+    long long m = 0;
+    for (int r = 0; r < NR; ++r) m = shift(r) < m ? shift(r) : m;
+    return m;
+}
+
+// Factors of reaction R over species [S0, S1) at the multi-index v (indexed from S0): src at v - nu
+// (TRANS: at v, with the target v + nu checked), 0 when that leaves the box; diag at v.
+template <int R, int S0, int S1, bool TRANS, int M>
+__device__ __forceinline__ void span_factors(const double *tab, const int (&v)[M], double &src, double &diag) {
+    double d = 1.0, sv = 1.0;
+    bool ok = true;
+#pragma unroll
+    for (int s = S0; s < S1; ++s) {
+        const int xs = v[s - S0];
+        if (nu(R, s) != 0) {
+            int w = TRANS ? xs + nu(R, s) : xs - nu(R, s);
+            ok = ok && w >= 0 && w < ext(s);
+            if (kind(R, s) != 0) {
+                d *= factor<R>(tab, s, xs);
+                if (!TRANS) {
+                    w = w < 0 ? 0 : (w >= ext(s) ? ext(s) - 1 : w);
+                    sv *= factor<R>(tab, s, w);
+                }
+            }
+        } else if (kind(R, s) != 0) {
+            const double f = factor<R>(tab, s, xs);
+            d *= f;
+            sv *= f;
+        }
+    }
+    diag = d;
+    src = ok ? (TRANS ? d : sv) : 0.0;
+}
+
+struct RowRegs {
+    double A[VP][NT];  // per term
+    double E[VP][NR];  // per reaction with outer diagonal factors
+    double D0[VP];
+};
+
+template <int R, bool TRANS>
+__device__ __forceinline__ void chunk_prologue(const CufspKronRtcArgs &a, double alpha, const double *tab,
+                                               const int (&xi)[KI], int v, RowRegs &g) {
+    if constexpr (R < NR) {
+        double src, diag;
+        span_factors<R, 0, KI, TRANS, KI>(tab, xi, src, diag);
+        const double c = alpha * a.coef[R];
+        if constexpr (term_owner(R) == R) {
+            g.A[v][term_of(R)] = c * src;
+        } else {
+            g.A[v][term_of(R)] = fma(c, src, g.A[v][term_of(R)]);
+        }
+        if constexpr (outer_diag_one(R)) {
+            g.D0[v] = fma(c, diag, g.D0[v]);
+        } else {
+            g.E[v][R] = c * diag;
+        }
+        chunk_prologue<R + 1, TRANS>(a, alpha, tab, xi, v, g);
+    }
+}
+
+template <int R, bool TRANS>
+__device__ __forceinline__ void row_words(const double *tab, const int (&z)[NO], double (&G)[NR], double (&Gd)[NR]) {
+    if constexpr (R < NR) {
+        if constexpr (!outer_src_one(R) || !outer_diag_one(R)) {
+            double src, diag;
+            span_factors<R, KI, NS, TRANS, NO>(tab, z, src, diag);
+            G[R] = src;
+            Gd[R] = diag;
+        }
+        row_words<R + 1, TRANS>(tab, z, G, Gd);
+    }
+}
+
+// Gathers of terms T0 .. T0 + RC - 1 (the sources of term T at i - d, d the shift of its owner).
+template <int T0, int T, bool TRANS, bool SAFE>
+__device__ __forceinline__ void rows_load(const double *__restrict__ x, const long long (&i)[VP], double (&q)[RC][VP]) {
+    if constexpr (T < NT && T < T0 + RC) {
+        constexpr long long D = shift(term_rep(T));
+#pragma unroll
+        for (int v = 0; v < VP; ++v) {
+            long long j = TRANS ? i[v] + D : i[v] - D;
+            if (!SAFE) j = clamp_index(j);
+            q[T - T0][v] = __ldg(x + j);
+        }
+        rows_load<T0, T + 1, TRANS, SAFE>(x, i, q);
+    }
+}
+
+template <int T0, int T>
+__device__ __forceinline__ void rows_acc(const RowRegs &g, const double (&G)[NR], const double (&q)[RC][VP],
+                                         double (&acc)[VP]) {
+    if constexpr (T < NT && T < T0 + RC) {
+        constexpr int R = term_rep(T);
+#pragma unroll
+        for (int v = 0; v < VP; ++v) {
+            if constexpr (outer_src_one(R)) {
+                acc[v] = fma(g.A[v][T], q[T - T0][v], acc[v]);
+            } else {
+                acc[v] = fma(g.A[v][T] * G[R], q[T - T0][v], acc[v]);
+            }
+        }
+        rows_acc<T0, T + 1>(g, G, q, acc);
+    }
+}
+
+template <int T0, bool TRANS, bool SAFE>
+__device__ __forceinline__ void rows_all(const double *__restrict__ x, const RowRegs &g, const double (&G)[NR],
+                                         const long long (&i)[VP], double (&acc)[VP]) {
+    if constexpr (T0 < NT) {
+        double q[RC][VP];
+        rows_load<T0, T0, TRANS, SAFE>(x, i, q);
+        rows_acc<T0, T0>(g, G, q, acc);
+        rows_all<T0 + RC, TRANS, SAFE>(x, g, G, i, acc);
+    }
+}
+
+template <int R>
+__device__ __forceinline__ void rows_diag(const RowRegs &g, const double (&Gd)[NR], double (&dg)[VP]) {
+    if constexpr (R < NR) {
+        if constexpr (!outer_diag_one(R)) {
+#pragma unroll
+            for (int v = 0; v < VP; ++v) dg[v] = fma(g.E[v][R], Gd[R], dg[v]);
+        }
+        rows_diag<R + 1>(g, Gd, dg);
+    }
+}
+
+template <bool ACCUM, bool TRANS>
+__device__ __forceinline__ void kron_rows(const CufspKronRtcArgs &a, const double *__restrict__ x,
+                                          double *__restrict__ y) {
+    if (a.d_skip && *a.d_skip) return;
+    const double *__restrict__ tab = a.tables;
+    const double alpha = a.d_alpha ? __ldg(a.d_alpha) : 1.0;
+    const int lane = threadIdx.x & 31;
+    const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    const long long total = (a.q_end - a.q_begin) * NCH;
+    constexpr long long DMAX = TRANS ? -shift_min() : shift_max();  // largest amount subtracted
+    constexpr long long DMIN = TRANS ? -shift_max() : shift_min();
+    long long cur = -1;
+    RowRegs g;
+    long long pos[VP];
+    bool act[VP];
+    // The chunks of a warp's (row, chunk) pairs repeat with period NCH: when the warp count is a
+    // multiple of NCH the prologue runs once.
+    for (long long t = gw; t < total; t += nw) {
+        const long long ch = t % NCH;
+        const long long q = a.q_begin + t / NCH;
+        if (ch != cur) {
+            cur = ch;
+#pragma unroll
+            for (int v = 0; v < VP; ++v) {
+                pos[v] = ch * (32 * VP) + v * 32 + lane;
+                act[v] = pos[v] < LEN;
+                long long rem = act[v] ? pos[v] : LEN - 1;
+                int xi[KI];
+#pragma unroll
+                for (int s = 0; s < KI; ++s) {
+                    const long long qq = rem / ext(s);
+                    xi[s] = (int)(rem - qq * ext(s));
+                    rem = qq;
+                }
+                g.D0[v] = 0.0;
+                chunk_prologue<0, TRANS>(a, alpha, tab, xi, v, g);
+            }
+        }
+        int z[NO];
+        {
+            long long rem = q;
+#pragma unroll
+            for (int s = KI; s < NS; ++s) {
+                if (s == NS - 1) {
+                    z[s - KI] = (int)rem;
+                } else {
+                    const long long qq = rem / ext(s);
+                    z[s - KI] = (int)(rem - qq * ext(s));
+                    rem = qq;
+                }
+            }
+        }
+        double G[NR], Gd[NR];
+        row_words<0, TRANS>(tab, z, G, Gd);
+        long long i[VP];
+        double xv[VP], yv[VP], acc[VP], dg[VP];
+#pragma unroll
+        for (int v = 0; v < VP; ++v) {
+            i[v] = q * LEN + (act[v] ? pos[v] : 0);
+            xv[v] = __ldg(x + i[v]);
+            yv[v] = (ACCUM && act[v]) ? __ldcs(y + i[v]) : 0.0;
+            acc[v] = 0.0;
+            dg[v] = g.D0[v];
+        }
+        const bool safe = q * LEN >= DMAX && (q + 1) * LEN - 1 - DMIN <= N - 1;
+        if (safe) {
+            rows_all<0, TRANS, true>(x, g, G, i, acc);
+        } else {
+            rows_all<0, TRANS, false>(x, g, G, i, acc);
+        }
+        rows_diag<0>(g, Gd, dg);
+#pragma unroll
+        for (int v = 0; v < VP; ++v) {
+            if (act[v]) {
+                double r = fma(-dg[v], xv[v], acc[v]);
+                if (ACCUM) r += yv[v];
+                __stcs(y + i[v], r);
+            }
+        }
+    }
+}
+
+}  // namespace cufsp_kron
+
+extern "C" __global__ void __launch_bounds__(256, CUFSP_KRON_ROWS_MINB) cufsp_kron_rows_accum(
+    const CufspKronRtcArgs a, const double *__restrict__ x, double *__restrict__ y) {
+    cufsp_kron::kron_rows<true, false>(a, x, y);
+}
+
+extern "C" __global__ void __launch_bounds__(256, CUFSP_KRON_ROWS_MINB) cufsp_kron_rows_set(
+    const CufspKronRtcArgs a, const double *__restrict__ x, double *__restrict__ y) {
+    cufsp_kron::kron_rows<false, false>(a, x, y);
+}
+
+extern "C" __global__ void __launch_bounds__(256, CUFSP_KRON_ROWS_MINB) cufsp_kron_rowsT_set(
+    const CufspKronRtcArgs a, const double *__restrict__ x, double *__restrict__ y) {
+    cufsp_kron::kron_rows<false, true>(a, x, y);
 }
 
 #endif  // __CUDACC_RTC__

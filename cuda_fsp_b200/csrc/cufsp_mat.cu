@@ -148,6 +148,16 @@ extern "C" cufsp_status cufsp_mat_apply(cufsp_mat *A, double t, const double *co
     return mat_apply(A, A->coef_buf.data(), alpha, nullptr, nullptr, x, beta != 0.0, y, (cudaStream_t)stream);
 }
 
+extern "C" cufsp_status cufsp_mat_apply_transpose(cufsp_mat *A, double t, const double *coefs, double alpha,
+                                                  const double *x, double *y, cufsp_stream_t stream) {
+    if (!A || !x || !y) return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_mat_apply_transpose: NULL argument");
+    if (x == y) return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_mat_apply_transpose: x and y must not alias");
+    if (!std::isfinite(alpha)) return set_error(CUFSP_ERR_NONFINITE, "cufsp_mat_apply_transpose: alpha is NaN/Inf");
+    cufsp_status s = mat_coefs(A, t, coefs, A->coef_buf);
+    if (s != CUFSP_SUCCESS) return s;
+    return mat_apply_transpose(A, A->coef_buf.data(), alpha, nullptr, nullptr, x, y, (cudaStream_t)stream);
+}
+
 extern "C" cufsp_status cufsp_mat_action(cufsp_mat *A, double t, const double *x, double *y, cufsp_stream_t stream) {
     return cufsp_mat_apply(A, t, nullptr, 1.0, x, 1.0, y, stream);
 }

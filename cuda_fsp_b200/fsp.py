@@ -160,6 +160,15 @@ class FSPMat:
         _lib.check(self._lib, self._lib.cufsp_mat_apply(self._h, float(t), cp, float(alpha), _ptr(x), float(beta),
                                                         _ptr(y), _stream(stream)), "cufsp_mat_apply")
 
+    def apply_transpose(self, x, y, coefs=None, alpha: float = 1.0, t: float = 0.0, stream=None) -> None:
+        """y = alpha * A^T x (KRONECKER format; the adjoint solves' operator)."""
+        cp = None
+        if coefs is not None:
+            carr = np.ascontiguousarray(np.asarray(coefs, np.float64).reshape(self.nr))
+            cp = carr.ctypes.data_as(C.POINTER(C.c_double))
+        _lib.check(self._lib, self._lib.cufsp_mat_apply_transpose(self._h, float(t), cp, float(alpha), _ptr(x), _ptr(y),
+                                                                  _stream(stream)), "cufsp_mat_apply_transpose")
+
     def action_host(self, t: float, x_host, y_host) -> None:
         """y_host += A(t) x_host on host buffers (pinned for full speed); synchronous."""
         def hp(a):

@@ -117,6 +117,12 @@ cufsp_status cufsp_mat_action(cufsp_mat *A, double t, const double *x, double *y
 cufsp_status cufsp_mat_apply(cufsp_mat *A, double t, const double *coefs, double alpha, const double *x,
                              double beta, double *y, cufsp_stream_t stream);
 
+/* y = alpha A(t)^T x (overwrite), the operator of the adjoint solves; KRONECKER generators only
+ * (no counterpart in the reference, whose solvers never apply A^T).  coefs as in cufsp_mat_apply;
+ * x and y must not alias.  Asynchronous on `stream`. */
+cufsp_status cufsp_mat_apply_transpose(cufsp_mat *A, double t, const double *coefs, double alpha, const double *x,
+                                       double *y, cufsp_stream_t stream);
+
 /* FSPMat::action with HOST buffers: y_host += A(t) x_host.  Copies in, computes and copies out in
  * a pipeline of slabs on internal streams; returns after y_host is written (synchronous).
  * x_host / y_host should be pinned (cudaHostAlloc) for full PCIe bandwidth. */
