@@ -329,6 +329,9 @@ struct KronData {
     int rows_k = 1;               // inner species
     int64_t rows_L = 1;           // inner positions per row
     int rows_grid = 0;
+    // slab kernels of the same module (cufsp_kron_slab_*): the row kernels' arithmetic on TMA-staged rows
+    int slab_grid = 0, slab_threads = 0;
+    size_t slab_smem = 0;
     const ModelHost *model = nullptr;  // the generator's model (outlives this object), for the lazy build
 };
 
@@ -561,13 +564,51 @@ static void kron_build_rtc(const ModelHost &m, KronData *kd) {
     const int rminb = std::max(1, std::min(8, env_or("CUFSP_KRON_ROWS_MINB", rv == 4 ? 1 : (rv == 2 ? 2 : 3))));
     kd->rows_k = rk;
     kd->rows_L = rL;
+    // Slab kernels (rows staged by TMA): rows of 64..2048 positions (even: 16-byte copies), reactions
+    // moving the row by at most 2, at least 8 rows per CTA of a full grid; up to 4 positions per thread.
+    int slab_h = 0, slab_g = 0;
+    const int64_t n_rows = m.n / rL;
+    bool slab = env_or("CUFSP_KRON_SLAB", 1) != 0 && ns >= 2 && rL % 2 == 0 && rL >= 64 && rL <= 2048 &&
+                n_rows >= 8LL * device_info().sm_count;
+    for (int r = 0; r < nr && slab; ++r) {
+        int64_t dp = 0, st2 = 1;
+        for (int s2 = 0; s2 < rk; ++s2) {
+            dp += (int64_t)m.nu[(size_t)r * ns + s2] * st2;
+            st2 *= (int64_t)m.bounds[s2] + 1;
+        }
+        int64_t dfull = 0;
+        for (int s2 = 0; s2 < ns; ++s2) dfull += (int64_t)m.nu[(size_t)r * ns + s2] * stride[s2];
+        const int64_t dq = (dfull - dp) / rL;
+        if (std::llabs(dq) > 2 || std::llabs(dp) > 512) slab = false;
+        slab_h = std::max<int>(slab_h, (int)std::llabs(dq));
+        slab_g = std::max<int>(slab_g, (int)std::llabs(dp));
+    }
+    slab_g = (slab_g + 1) & ~1;
+    const int slab_vs = (int)std::max<int64_t>(1, std::min<int64_t>(4, rL / 128));  // >= 4 warps per CTA
+    const int slab_t = (int)((rL + 32LL * slab_vs - 1) / (32LL * slab_vs)) * 32;
+    const int slab_minb = slab_t <= 256 ? 2 : 1;
+    const int64_t stage_bytes = 8 * (rL + 2LL * slab_g + ((rL + 1) & ~1LL));
+    const int64_t budget = slab_minb == 2 ? 110 * 1024 : 200 * 1024;
+    int slab_s = (int)std::min<int64_t>(8, budget / stage_bytes);
+    slab_s = std::min(slab_s, env_or("CUFSP_KRON_SLAB_S", slab_s));
+    if (slab_s < 2 * slab_h + 2) slab = false;
+    kd->slab_smem = slab ? (size_t)slab_s * (size_t)stage_bytes : 0;
+    kd->slab_threads = slab_t;
     std::ostringstream o;
     o << "#define CUFSP_KRON_MINB " << minb << "\n#define CUFSP_KRON_RTC_MAX_R " << CUFSP_KRON_RTC_MAX_R
       << "\n#define CUFSP_KRON_NS " << ns << "\n#define CUFSP_KRON_NR " << nr << "\n#define CUFSP_KRON_N " << m.n
       << "LL\n#define CUFSP_KRON_CHUNK " << chunk << "\n#define CUFSP_KRON_TS " << std::max<size_t>(1, packed.size())
       << "\n#define CUFSP_KRON_TAB_SMEM " << (tab_smem ? 1 : 0) << "\n#define CUFSP_KRON_K " << rk
       << "\n#define CUFSP_KRON_V " << rv << "\n#define CUFSP_KRON_L " << rL << "LL\n#define CUFSP_KRON_RCHUNK " << rchunk
-      << "\n#define CUFSP_KRON_ROWS_MINB " << rminb << "\nnamespace cufsp_kron {\n";
+      << "\n#define CUFSP_KRON_ROWS_MINB " << rminb << "\n#define CUFSP_KRON_SLAB " << (slab ? 1 : 0)
+      << "\n#define CUFSP_KRON_SLAB_T " << slab_t << "\n#define CUFSP_KRON_SLAB_VS " << slab_vs
+      << "\n#define CUFSP_KRON_SLAB_S " << slab_s << "\n#define CUFSP_KRON_SLAB_H " << slab_h
+      << "\n#define CUFSP_KRON_SLAB_G " << slab_g << "\n#define CUFSP_KRON_SLAB_MINB " << slab_minb;
+    // Bounded waits of the slab kernels: 2^20 tries unless CUFSP_KRON_SLAB_WAIT_TRIES asks for fewer
+    // (the watchdog's own test: 0 makes every wait before a row give up at once).
+    if (const char *ev = getenv("CUFSP_KRON_SLAB_WAIT_TRIES"))
+        o << "\n#define CUFSP_KRON_SLAB_WAIT_TRIES " << std::max(0, std::min(1 << 20, atoi(ev)));
+    o << "\nnamespace cufsp_kron {\n";
     o << "__device__ __forceinline__ constexpr int ext(int s) {";
     for (int s = 0; s < ns; ++s) o << " if (s == " << s << ") return " << m.bounds[s] + 1 << ";";
     o << " return 1; }\n";
@@ -590,10 +631,10 @@ static void kron_build_rtc(const ModelHost &m, KronData *kd) {
     }
     o << " return 0; }\n}\n";
     std::string why;
-    auto mod = rtc_module(o.str() + kKronRtcSource,
-                          {"cufsp_kron_mv_accum", "cufsp_kron_mv_set", "cufsp_kron_mvT_set", "cufsp_kron_rows_accum",
-                           "cufsp_kron_rows_set", "cufsp_kron_rowsT_set"},
-                          why);
+    std::vector<std::string> names = {"cufsp_kron_mv_accum",   "cufsp_kron_mv_set",   "cufsp_kron_mvT_set",
+                                      "cufsp_kron_rows_accum", "cufsp_kron_rows_set", "cufsp_kron_rowsT_set"};
+    if (slab) names.insert(names.end(), {"cufsp_kron_slab_accum", "cufsp_kron_slab_set", "cufsp_kron_slabT_set"});
+    auto mod = rtc_module(o.str() + kKronRtcSource, names, why);
     if (!mod) {
         kd->rtc_why = why;
         return;
@@ -622,6 +663,21 @@ static void kron_build_rtc(const ModelHost &m, KronData *kd) {
         cudaGetLastError();
         kd->rows_forward = kd->rows_transpose = false;
         return;
+    }
+    // Slab kernels: one CTA per row segment, as many segments as CTAs fit, at least 8 rows each.
+    kd->slab_grid = 0;
+    if (slab) {
+        int socc = 0;
+        bool sok = true;
+        for (int k = 6; k < 9 && sok; ++k)
+            sok = cudaFuncSetAttribute((const void *)mod->kernels[k], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)kd->slab_smem) == cudaSuccess;
+        if (sok && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&socc, (const void *)mod->kernels[6], slab_t,
+                                                                 kd->slab_smem) == cudaSuccess &&
+            socc >= 1 && (kd->h_err || (kd->h_err = watch_word_alloc(&kd->d_err)))) {
+            kd->slab_grid = (int)std::min<int64_t>((int64_t)device_info().sm_count * std::min(socc, 8), n_rows / 8);
+        }
+        cudaGetLastError();
     }
     const int64_t nch = (rL + 32LL * rv - 1) / (32LL * rv);
     const int64_t resident = (int64_t)device_info().sm_count * rocc;
@@ -870,6 +926,11 @@ cufsp_status kron_prepare(KronData *k, const double *coefs, cudaStream_t st, boo
 
 std::string kron_describe(const KronData *k) {
     if (k->plane) return plane_description(k->plane);
+    if (k->rows_forward && k->rtc && k->slab_grid > 0)
+        return "slab kernel specialised for the network and box (NVRTC, sm_100a, TMA ring): " +
+               std::to_string(k->rows_k) + " inner species, rows of " + std::to_string(k->rows_L) + " positions, " +
+               std::to_string(k->slab_grid) + " CTAs x " + std::to_string(k->slab_threads) + " threads, " +
+               std::to_string(k->slab_smem) + " B smem; plane kernel not used: " + k->plane_why;
     if (k->rows_forward && k->rtc && k->rows_grid > 0)
         return "row kernel specialised for the network and box (NVRTC, sm_100a): " + std::to_string(k->rows_k) +
                " inner species, rows of " + std::to_string(k->rows_L) + " positions, " + std::to_string(k->rows_grid) +
@@ -943,6 +1004,13 @@ static cufsp_status rows_launch(KronData *kd, const double *coefs, double alpha,
     r.q_end = kd->n / kd->rows_L;
     for (int k = 0; k < kd->nr; ++k) r.coef[k] = alpha * coefs[k];
     void *args[] = {&r, (void *)&x, (void *)&y};
+    // The slab kernel copies whole rows with 16-byte bulk copies: x and y must be 16-byte aligned.
+    if (kd->slab_grid > 0 && ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) % 16) == 0) {
+        r.err = kd->d_err;
+        CUFSP_CUDA_TRY(cudaLaunchKernel((const void *)kd->rtc->kernels[which + 3], dim3(kd->slab_grid),
+                                        dim3(kd->slab_threads), args, kd->slab_smem, st));
+        return CUFSP_SUCCESS;
+    }
     CUFSP_CUDA_TRY(cudaLaunchKernel((const void *)kd->rtc->kernels[which], dim3(kd->rows_grid), dim3(256), args, 0, st));
     return CUFSP_SUCCESS;
 }

@@ -25,7 +25,8 @@ struct CufspKronRtcArgs {
     const double *d_alpha;  // nullable device scalar multiplying every coefficient
     const int *d_skip;      // nullable: return at once when *d_skip != 0
     long long i_begin, i_end;
-    long long q_begin, q_end;  // row range of the row kernels (cufsp_kron_rows_*)
+    long long q_begin, q_end;  // row range of the row and slab kernels
+    int *err;                  // watchdog word of the slab kernels (set when a bounded wait expired)
     double coef[CUFSP_KRON_RTC_MAX_R];  // alpha * c_r
 };
 
@@ -345,15 +346,17 @@ __device__ __forceinline__ void span_factors(const double *tab, const int (&v)[M
     src = ok ? (TRANS ? d : sv) : 0.0;
 }
 
-struct RowRegs {
-    double A[VP][NT];  // per term
-    double E[VP][NR];  // per reaction with outer diagonal factors
-    double D0[VP];
+template <int V>
+struct PosRegs {
+    double A[V][NT];  // per term
+    double E[V][NR];  // per reaction with outer diagonal factors
+    double D0[V];
 };
+using RowRegs = PosRegs<VP>;
 
-template <int R, bool TRANS>
+template <int R, bool TRANS, int V>
 __device__ __forceinline__ void chunk_prologue(const CufspKronRtcArgs &a, double alpha, const double *tab,
-                                               const int (&xi)[KI], int v, RowRegs &g) {
+                                               const int (&xi)[KI], int v, PosRegs<V> &g) {
     if constexpr (R < NR) {
         double src, diag;
         span_factors<R, 0, KI, TRANS, KI>(tab, xi, src, diag);
@@ -368,7 +371,7 @@ __device__ __forceinline__ void chunk_prologue(const CufspKronRtcArgs &a, double
         } else {
             g.E[v][R] = c * diag;
         }
-        chunk_prologue<R + 1, TRANS>(a, alpha, tab, xi, v, g);
+        chunk_prologue<R + 1, TRANS, V>(a, alpha, tab, xi, v, g);
     }
 }
 
@@ -428,14 +431,38 @@ __device__ __forceinline__ void rows_all(const double *__restrict__ x, const Row
     }
 }
 
-template <int R>
-__device__ __forceinline__ void rows_diag(const RowRegs &g, const double (&Gd)[NR], double (&dg)[VP]) {
+template <int R, int V>
+__device__ __forceinline__ void rows_diag(const PosRegs<V> &g, const double (&Gd)[NR], double (&dg)[V]) {
     if constexpr (R < NR) {
         if constexpr (!outer_diag_one(R)) {
 #pragma unroll
-            for (int v = 0; v < VP; ++v) dg[v] = fma(g.E[v][R], Gd[R], dg[v]);
+            for (int v = 0; v < V; ++v) dg[v] = fma(g.E[v][R], Gd[R], dg[v]);
         }
-        rows_diag<R + 1>(g, Gd, dg);
+        rows_diag<R + 1, V>(g, Gd, dg);
+    }
+}
+
+// Decode inner position p (< LEN) into the inner multi-index.
+__device__ __forceinline__ void inner_decode(long long p, int (&xi)[KI]) {
+#pragma unroll
+    for (int s = 0; s < KI; ++s) {
+        const long long qq = p / ext(s);
+        xi[s] = (int)(p - qq * ext(s));
+        p = qq;
+    }
+}
+
+// Decode row q into the outer multi-index.
+__device__ __forceinline__ void outer_decode(long long q, int (&z)[NO]) {
+#pragma unroll
+    for (int s = KI; s < NS; ++s) {
+        if (s == NS - 1) {
+            z[s - KI] = (int)q;
+        } else {
+            const long long qq = q / ext(s);
+            z[s - KI] = (int)(q - qq * ext(s));
+            q = qq;
+        }
     }
 }
 
@@ -475,7 +502,7 @@ __device__ __forceinline__ void kron_rows(const CufspKronRtcArgs &a, const doubl
                     rem = qq;
                 }
                 g.D0[v] = 0.0;
-                chunk_prologue<0, TRANS>(a, alpha, tab, xi, v, g);
+                chunk_prologue<0, TRANS, VP>(a, alpha, tab, xi, v, g);
             }
         }
         int z[NO];
@@ -510,7 +537,7 @@ __device__ __forceinline__ void kron_rows(const CufspKronRtcArgs &a, const doubl
         } else {
             rows_all<0, TRANS, false>(x, g, G, i, acc);
         }
-        rows_diag<0>(g, Gd, dg);
+        rows_diag<0, VP>(g, Gd, dg);
 #pragma unroll
         for (int v = 0; v < VP; ++v) {
             if (act[v]) {
@@ -538,6 +565,233 @@ extern "C" __global__ void __launch_bounds__(256, CUFSP_KRON_ROWS_MINB) cufsp_kr
     const CufspKronRtcArgs a, const double *__restrict__ x, double *__restrict__ y) {
     cufsp_kron::kron_rows<false, true>(a, x, y);
 }
+
+// ---- Slab kernels: the row kernels' arithmetic on rows staged in shared memory by TMA ----------
+// For networks whose reactions move the row index q by at most H rows (|dq| <= H) and whose rows fit
+// shared memory: a CTA owns a segment of whole rows [q0, q1) and streams rows q0 - H .. q1 - 1 + H
+// through a ring of SS stages, one bulk copy (cp.async.bulk + mbarrier complete_tx) per row of x
+// (and of y, for the rows it computes, in the accumulate form), issued by one thread as stages free
+// up.  Row q is computed from the stages of rows q - H .. q + H: every gather is a shared-memory load
+// at a compile-time offset, and every x value crosses HBM once per segment (plus 2H halo rows).  Each
+// staged x row has GD zero guard doubles on both sides, so inner sources outside the row read 0
+// (their factor is 0 as well) without a clamp.  Rows outside the box are never copied: their stage
+// arrives empty and their outer factor is 0.  Every mbarrier wait is bounded; on expiry the CTA
+// drains its copies (bounded), sets the watchdog word and leaves its rows unwritten.
+
+#if CUFSP_KRON_SLAB
+namespace cufsp_kron {
+
+constexpr int ST = CUFSP_KRON_SLAB_T;   // threads per CTA
+constexpr int VS = CUFSP_KRON_SLAB_VS;  // positions per thread, ST apart
+constexpr int SS = CUFSP_KRON_SLAB_S;   // ring stages
+constexpr int HB = CUFSP_KRON_SLAB_H;   // row halo on each side
+constexpr int GD = CUFSP_KRON_SLAB_G;   // zero guard doubles on each side of a staged x row (even)
+constexpr int PITCH = (int)LEN + 2 * GD;
+constexpr int SD = PITCH + (int)((LEN + 1) & ~1LL);  // stage: guarded x row, then the y row
+constexpr long long QN = N / LEN;                    // rows in the box
+#ifndef CUFSP_KRON_SLAB_WAIT_TRIES
+#define CUFSP_KRON_SLAB_WAIT_TRIES (1 << 20)
+#endif
+
+__device__ __forceinline__ constexpr long long istride(int s) {
+    long long st = 1;
+    for (int u = 0; u < s; ++u) st *= ext(u);
+    return st;
+}
+__device__ __forceinline__ constexpr long long inner_shift(int r) {
+    long long d = 0;
+    for (int s = 0; s < KI; ++s) d += (long long)nu(r, s) * istride(s);
+    return d;
+}
+__device__ __forceinline__ constexpr long long row_shift(int r) { return (shift(r) - inner_shift(r)) / LEN; }
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long *bar, unsigned parity, int tries) {
+    for (int it = 0; it < tries; ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+__device__ __forceinline__ void tma_load(void *dst, const void *src, unsigned bytes, unsigned long long *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+// acc += sum over terms of A_T(p) G_T(q) x[source]; rowp[k] is the staged x row of row q - HB + k.
+template <int T, bool TRANS>
+__device__ __forceinline__ void slab_terms(const double *const (&rowp)[2 * HB + 1], const PosRegs<VS> &g,
+                                           const double (&G)[NR], const int (&pos)[VS], double (&acc)[VS]) {
+    if constexpr (T < NT) {
+        constexpr int R = term_rep(T);
+        constexpr int DQ = TRANS ? -(int)row_shift(R) : (int)row_shift(R);  // source row q - DQ
+        constexpr int DP = TRANS ? -(int)inner_shift(R) : (int)inner_shift(R);
+        const double *src = rowp[HB - DQ] + (GD - DP);
+#pragma unroll
+        for (int v = 0; v < VS; ++v) {
+            const double xs = src[pos[v]];
+            if constexpr (outer_src_one(R)) {
+                acc[v] = fma(g.A[v][T], xs, acc[v]);
+            } else {
+                acc[v] = fma(g.A[v][T] * G[R], xs, acc[v]);
+            }
+        }
+        slab_terms<T + 1, TRANS>(rowp, g, G, pos, acc);
+    }
+}
+
+template <bool ACCUM, bool TRANS>
+__device__ __forceinline__ void kron_slab(const CufspKronRtcArgs &a, const double *__restrict__ x,
+                                          double *__restrict__ y) {
+    extern __shared__ __align__(128) double smem[];
+    __shared__ __align__(8) unsigned long long bars[SS];
+    __shared__ int failed;
+    if (a.d_skip && *a.d_skip) return;
+    const long long nrows = a.q_end - a.q_begin;
+    const long long seg = (nrows + gridDim.x - 1) / gridDim.x;
+    const long long q0 = a.q_begin + (long long)blockIdx.x * seg;
+    const long long q1 = min(a.q_end, q0 + seg);
+    if (q0 >= q1) return;  // whole CTA leaves before any barrier or copy
+    const int tid = threadIdx.x;
+    for (int k = tid; k < SS * SD; k += ST) smem[k] = 0.0;  // guards and never-copied rows stay zero
+    if (tid == 0) {
+        for (int k = 0; k < SS; ++k) mbar_init(bars + k, 1);
+        fence_mbar_init();
+        failed = 0;
+    }
+    fence_proxy_async();
+    __syncthreads();
+
+    // Row p >= pbase lives in stage (p - pbase) % SS, phase parity ((p - pbase) / SS) & 1.
+    const long long pbase = q0 - HB, plast = q1 - 1 + HB;
+    auto stage = [&](long long p) { return smem + ((p - pbase) % SS) * SD; };
+    auto bar = [&](long long p) { return bars + (p - pbase) % SS; };
+    auto parity = [&](long long p) { return (unsigned)(((p - pbase) / SS) & 1); };
+    auto issue = [&](long long p) {  // one thread
+        if (p < 0 || p >= QN) {  // outside the box: the stage arrives without a copy
+            mbar_expect_tx(bar(p), 0u);
+            return;
+        }
+        const bool own = ACCUM && p >= q0 && p < q1;
+        double *st = stage(p);
+        mbar_expect_tx(bar(p), (unsigned)(LEN * 8 * (own ? 2 : 1)));
+        tma_load(st + GD, x + p * LEN, (unsigned)(LEN * 8), bar(p));
+        if (own) tma_load(st + PITCH, y + p * LEN, (unsigned)(LEN * 8), bar(p));
+    };
+    long long issued = pbase - 1;
+    if (tid == 0) {
+        const long long stop = min(plast, pbase + SS - 1);
+        for (long long p = pbase; p <= stop; ++p) issue(p);
+        issued = stop;
+    }
+
+    // inner factors of the thread's positions (registers, fixed for the launch)
+    const double *__restrict__ tab = a.tables;
+    const double alpha = a.d_alpha ? __ldg(a.d_alpha) : 1.0;
+    PosRegs<VS> g;
+    int pos[VS];
+    bool act[VS];
+#pragma unroll
+    for (int v = 0; v < VS; ++v) {
+        pos[v] = v * ST + tid;
+        act[v] = pos[v] < LEN;
+        int xi[KI];
+        inner_decode(act[v] ? pos[v] : LEN - 1, xi);
+        g.D0[v] = 0.0;
+        chunk_prologue<0, TRANS, VS>(a, alpha, tab, xi, v, g);
+        if (!act[v]) pos[v] = 0;  // idle position: reads stay inside the row, nothing is written
+    }
+
+    bool ok = true;
+    long long waited = pbase - 1;  // rows whose copies this thread has seen land
+    for (long long p = pbase; p < q0 + HB && ok; ++p) {
+        ok = mbar_wait_bounded(bar(p), parity(p), CUFSP_KRON_SLAB_WAIT_TRIES);
+        if (ok) waited = p;
+    }
+    for (long long q = q0; q < q1; ++q) {
+        if (ok) ok = mbar_wait_bounded(bar(q + HB), parity(q + HB), CUFSP_KRON_SLAB_WAIT_TRIES);
+        if (!ok) {
+            failed = 1;
+        } else {
+            waited = q + HB;
+            int z[NO];
+            outer_decode(q, z);
+            double G[NR], Gd[NR];
+            row_words<0, TRANS>(tab, z, G, Gd);
+            const double *rowp[2 * HB + 1];
+#pragma unroll
+            for (int k = 0; k <= 2 * HB; ++k) rowp[k] = stage(q - HB + k);
+            const double *xs = rowp[HB] + GD;
+            const double *ys = rowp[HB] + PITCH;
+            double xv[VS], acc[VS], dg[VS];
+#pragma unroll
+            for (int v = 0; v < VS; ++v) {
+                xv[v] = xs[pos[v]];
+                acc[v] = 0.0;
+                dg[v] = g.D0[v];
+            }
+            slab_terms<0, TRANS>(rowp, g, G, pos, acc);
+            rows_diag<0, VS>(g, Gd, dg);
+#pragma unroll
+            for (int v = 0; v < VS; ++v) {
+                if (act[v]) {
+                    double r = fma(-dg[v], xv[v], acc[v]);
+                    if (ACCUM) r += ys[pos[v]];
+                    __stcs(y + q * LEN + pos[v], r);
+                }
+            }
+        }
+        __syncthreads();  // the stage of row q - HB is consumed
+        if (failed) break;
+        if (tid == 0 && issued < plast) {
+            ++issued;
+            fence_proxy_async();
+            issue(issued);
+        }
+    }
+    if (tid == 0) {
+        // every issued copy must land before the CTA's shared memory is released
+        bool bad = failed != 0;
+        for (long long p = waited + 1; p <= issued; ++p)
+            if (!mbar_wait_bounded(bar(p), parity(p), 1 << 20)) bad = true;
+        if (bad && a.err) atomicExch(a.err, 1);
+    }
+}
+
+}  // namespace cufsp_kron
+
+extern "C" __global__ void __launch_bounds__(CUFSP_KRON_SLAB_T, CUFSP_KRON_SLAB_MINB) cufsp_kron_slab_accum(
+    const CufspKronRtcArgs a, const double *__restrict__ x, double *__restrict__ y) {
+    cufsp_kron::kron_slab<true, false>(a, x, y);
+}
+
+extern "C" __global__ void __launch_bounds__(CUFSP_KRON_SLAB_T, CUFSP_KRON_SLAB_MINB) cufsp_kron_slab_set(
+    const CufspKronRtcArgs a, const double *__restrict__ x, double *__restrict__ y) {
+    cufsp_kron::kron_slab<false, false>(a, x, y);
+}
+
+extern "C" __global__ void __launch_bounds__(CUFSP_KRON_SLAB_T, CUFSP_KRON_SLAB_MINB) cufsp_kron_slabT_set(
+    const CufspKronRtcArgs a, const double *__restrict__ x, double *__restrict__ y) {
+    cufsp_kron::kron_slab<false, true>(a, x, y);
+}
+#endif  // CUFSP_KRON_SLAB
 
 #endif  // __CUDACC_RTC__
 #endif  // CUFSP_KRON_RTC_CUH

@@ -133,3 +133,60 @@ def test_row_kernels_off(cuda, monkeypatch):
     monkeypatch.setenv("CUFSP_KRON_ROWS", "0")
     A = check_rows(models.gene_expression((1, 1, 1, 127, 127), time_varying=False), expect_rows=False)
     assert "k_kron_mv" in A.describe(), A.describe()
+
+
+def slab_case(case):
+    if case == "gene":  # rows of 8 x 16 = 128 positions, 1,200 rows
+        return models.gene_expression((1, 1, 1, 15, 1199), time_varying=False)
+    if case == "random4":  # rows of 64 positions
+        return random_network((3, 3, 3, 1299), 9, 17)
+    if case == "random5":  # rows of 72 positions
+        return random_network((2, 3, 1, 2, 1300), 7, 19)
+    m = random_network((15, 3, 1400), 6, 23)  # a change of 2 rows and one of 3 positions
+    m.nu[1] = (0, 0, -2)
+    m.nu[3] = (3, 0, 0)
+    return m
+
+
+@pytest.mark.parametrize("case", ["gene", "random4", "random5", "big_change"])
+def test_slab_kernels_match_oracle(cuda, case, monkeypatch):
+    """The slab kernels (rows streamed through shared memory by TMA bulk copies) on networks with
+    at least 8 rows per CTA of a full grid: forward in both forms and transposed, to the matvec bar."""
+    monkeypatch.delenv("CUFSP_KRON_ROWS", raising=False)
+    A = check_rows(slab_case(case))
+    assert "slab kernel" in A.describe(), A.describe()
+    assert A.watchdog() == 0
+
+
+def test_slab_falls_back_for_8_byte_aligned_vectors(cuda):
+    """Vectors only 8-byte aligned (a Krylov basis vector at an odd offset) take the row kernel."""
+    import torch
+    m = slab_case("gene")
+    A = FSPMat.from_model(m, MatrixFormat.KRONECKER)
+    assert "slab kernel" in A.describe(), A.describe()
+    csr = oracle.assemble_model(m)
+    rng = np.random.default_rng(5)
+    x = rng.uniform(0, 1, m.n_states)
+    c = m.coefs(0.0)
+    xb = torch.zeros(m.n_states + 1, dtype=torch.float64, device="cuda")
+    yb = torch.zeros(m.n_states + 1, dtype=torch.float64, device="cuda")
+    xb[1:] = dev(x)
+    A.apply(xb[1:], yb[1:], coefs=c)
+    err = np.abs(host(yb[1:]) - csr.spmv(c, x)).max()
+    assert err <= MATVEC_RTOL * csr.abs_spmv(c, x).max(), err
+
+
+def test_slab_watchdog(cuda, monkeypatch):
+    """CUFSP_KRON_SLAB_WAIT_TRIES=0 at creation compiles the slab kernels with zero tries for the
+    waits before each row, so every such wait gives up at once: the kernel drains its copies (with its
+    normal bound), sets the watchdog word and returns; the context stays usable."""
+    m = slab_case("gene")
+    monkeypatch.setenv("CUFSP_KRON_SLAB_WAIT_TRIES", "0")
+    A = FSPMat.from_model(m, MatrixFormat.KRONECKER)
+    monkeypatch.delenv("CUFSP_KRON_SLAB_WAIT_TRIES")
+    assert "slab kernel" in A.describe(), A.describe()
+    y = dev(np.zeros(m.n_states))
+    A.apply(dev(np.ones(m.n_states)), y, coefs=m.coefs(0.0))
+    assert A.watchdog() == 1
+    assert A.watchdog() == 0
+    check_rows(m)  # a normal generator of the same network
