@@ -606,6 +606,7 @@ static void kron_build_rtc(const ModelHost &m, KronData *kd) {
       << "\n#define CUFSP_KRON_SLAB_G " << slab_g << "\n#define CUFSP_KRON_SLAB_MINB " << slab_minb;
     // Bounded waits of the slab kernels: 2^20 tries unless CUFSP_KRON_SLAB_WAIT_TRIES asks for fewer
     // (the watchdog's own test: 0 makes every wait before a row give up at once).
+    if (env_or("CUFSP_KRON_SLAB_SHFL", 1) == 0) o << "\n#define CUFSP_KRON_SLAB_SHFL 0";
     if (const char *ev = getenv("CUFSP_KRON_SLAB_WAIT_TRIES"))
         o << "\n#define CUFSP_KRON_SLAB_WAIT_TRIES " << std::max(0, std::min(1 << 20, atoi(ev)));
     o << "\nnamespace cufsp_kron {\n";

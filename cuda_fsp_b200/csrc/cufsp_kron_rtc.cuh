@@ -592,6 +592,9 @@ constexpr long long QN = N / LEN;                    // rows in the box
 #ifndef CUFSP_KRON_SLAB_WAIT_TRIES
 #define CUFSP_KRON_SLAB_WAIT_TRIES (1 << 20)
 #endif
+#ifndef CUFSP_KRON_SLAB_SHFL
+#define CUFSP_KRON_SLAB_SHFL 1
+#endif
 
 __device__ __forceinline__ constexpr long long istride(int s) {
     long long st = 1;
@@ -635,25 +638,56 @@ __device__ __forceinline__ void tma_load(void *dst, const void *src, unsigned by
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
 
+// Leading species of extent 2 (binary switches) up to lane bit 4: the state index of such a species'
+// flip differs from the state's in one bit below 32, i.e. in the lane index (positions are
+// lane-contiguous and ST is a multiple of 32).
+__device__ __forceinline__ constexpr int binary_prefix() {
+    int b = 0;
+    while (b < KI && b < 5 && ext(b) == 2) ++b;
+    return b;
+}
+// Mask m when reaction r changes only one binary-prefix species s, by 1, and leaves the row alone: its
+// source, wherever its factor is nonzero, is the lane p ^ m (m = 2^s).
+__device__ __forceinline__ constexpr int flip_mask(int r) {
+    if (!CUFSP_KRON_SLAB_SHFL || row_shift(r) != 0) return 0;
+    int m = 0;
+    for (int s = 0; s < KI; ++s) {
+        if (nu(r, s) == 0) continue;
+        if (m != 0 || s >= binary_prefix() || (nu(r, s) != 1 && nu(r, s) != -1)) return 0;
+        m = 1 << s;
+    }
+    return m;
+}
+// The mask of the term owned by reaction R when every reaction of the term has that same mask (the
+// source then comes by a warp shuffle instead of a shared-memory load), else 0.
+__device__ __forceinline__ constexpr int xor_mask(int R) {
+    const int m = flip_mask(R);
+    for (int u = 0; u < NR && m != 0; ++u)
+        if (term_owner(u) == R && flip_mask(u) != m) return 0;
+    return m;
+}
+
 // acc += sum over terms of A_T(p) G_T(q) x[source]; rowp[k] is the staged x row of row q - HB + k.
 template <int T, bool TRANS>
 __device__ __forceinline__ void slab_terms(const double *const (&rowp)[2 * HB + 1], const PosRegs<VS> &g,
-                                           const double (&G)[NR], const int (&pos)[VS], double (&acc)[VS]) {
+                                           const double (&G)[NR], const int (&pos)[VS], const double (&xv)[VS],
+                                           double (&acc)[VS]) {
     if constexpr (T < NT) {
         constexpr int R = term_rep(T);
         constexpr int DQ = TRANS ? -(int)row_shift(R) : (int)row_shift(R);  // source row q - DQ
         constexpr int DP = TRANS ? -(int)inner_shift(R) : (int)inner_shift(R);
+        constexpr int XM = xor_mask(R);
         const double *src = rowp[HB - DQ] + (GD - DP);
 #pragma unroll
         for (int v = 0; v < VS; ++v) {
-            const double xs = src[pos[v]];
+            const double xs = XM ? __shfl_xor_sync(0xffffffffu, xv[v], XM) : src[pos[v]];
             if constexpr (outer_src_one(R)) {
                 acc[v] = fma(g.A[v][T], xs, acc[v]);
             } else {
                 acc[v] = fma(g.A[v][T] * G[R], xs, acc[v]);
             }
         }
-        slab_terms<T + 1, TRANS>(rowp, g, G, pos, acc);
+        slab_terms<T + 1, TRANS>(rowp, g, G, pos, xv, acc);
     }
 }
 
@@ -747,7 +781,7 @@ __device__ __forceinline__ void kron_slab(const CufspKronRtcArgs &a, const doubl
                 acc[v] = 0.0;
                 dg[v] = g.D0[v];
             }
-            slab_terms<0, TRANS>(rowp, g, G, pos, acc);
+            slab_terms<0, TRANS>(rowp, g, G, pos, xv, acc);
             rows_diag<0, VS>(g, Gd, dg);
 #pragma unroll
             for (int v = 0; v < VS; ++v) {

@@ -142,13 +142,23 @@ def slab_case(case):
         return random_network((3, 3, 3, 1299), 9, 17)
     if case == "random5":  # rows of 72 positions
         return random_network((2, 3, 1, 2, 1300), 7, 19)
+    if case == "binary":  # three binary switches lead (sources by warp shuffle where one flips alone)
+        m = random_network((1, 1, 1, 7, 1300), 10, 29)
+        m.nu[1] = (0, 0, -1, 0, 0)
+        m.nu[3] = (0, 1, 0, 0, 0)
+        m.nu[7] = (1, 0, 0, 0, 0)
+        m.nu[9] = (-1, 0, 0, 0, 0)
+        m.nu[2] = (1, -1, 0, 0, 0)  # the same flat shift as reaction 9, another source pattern
+        m.tables[2, 2:] = 1.0       # outer factors (and species 1) all ones: may share reaction 9's term
+        m.tables[9, 2:] = 1.0
+        return m
     m = random_network((15, 3, 1400), 6, 23)  # a change of 2 rows and one of 3 positions
     m.nu[1] = (0, 0, -2)
     m.nu[3] = (3, 0, 0)
     return m
 
 
-@pytest.mark.parametrize("case", ["gene", "random4", "random5", "big_change"])
+@pytest.mark.parametrize("case", ["gene", "random4", "random5", "binary", "big_change"])
 def test_slab_kernels_match_oracle(cuda, case, monkeypatch):
     """The slab kernels (rows streamed through shared memory by TMA bulk copies) on networks with
     at least 8 rows per CTA of a full grid: forward in both forms and transposed, to the matvec bar."""
