@@ -36,7 +36,7 @@ constexpr int kPThreads = 1024;
 constexpr int kPWarps = kPThreads / 32;
 constexpr int kKMax = 64;            // partial sums per CTA (>= CUFSP_MAX_KRYLOV)
 constexpr int kMaxTerms = 64;
-constexpr int kSpinLimit = 1 << 22;  // x __nanosleep(64): >= 0.27 s
+constexpr unsigned long long kWaitNs = 300ull * 1000 * 1000;  // a grid barrier gives up after 0.3 s
 
 struct PArgs {
     int64_t n;
@@ -64,6 +64,12 @@ struct PSmem {
     int ok;
 };
 
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
 __device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
     unsigned v;
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
@@ -75,21 +81,26 @@ __device__ __forceinline__ bool grid_sync(const PArgs &a, unsigned &epoch, int &
     __syncthreads();
     ++epoch;
     if (threadIdx.x == 0) {
-        __threadfence();
-        atomicAdd(a.bar, 1u);
+        // arrival with release semantics (the CTA's partial sums and w become visible first), then a
+        // tight acquire poll; a measured cooperative probe: 1.26 us per barrier over 148 CTAs, against
+        // 1.39-1.64 us for a fence, a relaxed atomic and 64 ns sleeps between polls.  The wait is
+        // bounded by the global timer (kWaitNs); the error word is looked at every 64 polls.
+        asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(a.bar), "r"(1u) : "memory");
         const unsigned target = epoch * gridDim.x;
         int ok = 1;
-        for (int it = 0; ld_acquire(a.bar) < target; ++it) {
-            if (it >= kSpinLimit) {
-                atomicExch(a.err, 1);
-                ok = 0;
-                break;
+        const unsigned long long t0 = global_ns();
+        for (int it = 1; ld_acquire(a.bar) < target; ++it) {
+            if ((it & 63) == 0) {
+                if (*(volatile int *)a.err) {  // another CTA gave up
+                    ok = 0;
+                    break;
+                }
+                if (global_ns() - t0 > kWaitNs) {
+                    atomicExch(a.err, 1);
+                    ok = 0;
+                    break;
+                }
             }
-            if (*(volatile int *)a.err) {  // another CTA gave up
-                ok = 0;
-                break;
-            }
-            __nanosleep(64);
         }
         __threadfence();
         ok_s = ok && *(volatile int *)a.err == 0;
