@@ -564,12 +564,12 @@ static void kron_build_rtc(const ModelHost &m, KronData *kd) {
     const int rminb = std::max(1, std::min(8, env_or("CUFSP_KRON_ROWS_MINB", rv == 4 ? 1 : (rv == 2 ? 2 : 3))));
     kd->rows_k = rk;
     kd->rows_L = rL;
-    // Slab kernels (rows staged by TMA): rows of 64..2048 positions (even: 16-byte copies), reactions
-    // moving the row by at most 2, at least 8 rows per CTA of a full grid; up to 4 positions per thread.
+    // Slab kernels (rows staged by TMA): rows of at least 64 positions (even: 16-byte copies), cut into
+    // tiles of at most 1024 positions (4 per thread); reactions moving the row by at most 2 and the
+    // position by at most 512; CTAs = tiles x row segments of at least 8 rows, enough to fill the SMs.
     int slab_h = 0, slab_g = 0;
     const int64_t n_rows = m.n / rL;
-    bool slab = env_or("CUFSP_KRON_SLAB", 1) != 0 && ns >= 2 && rL % 2 == 0 && rL >= 64 && rL <= 2048 &&
-                n_rows >= 8LL * device_info().sm_count;
+    bool slab = env_or("CUFSP_KRON_SLAB", 1) != 0 && ns >= 2 && rL % 2 == 0 && rL >= 64 && n_rows >= 8;
     for (int r = 0; r < nr && slab; ++r) {
         int64_t dp = 0, st2 = 1;
         for (int s2 = 0; s2 < rk; ++s2) {
@@ -585,13 +585,23 @@ static void kron_build_rtc(const ModelHost &m, KronData *kd) {
     }
     slab_g = (slab_g + 1) & ~1;
     const int slab_vs = (int)std::max<int64_t>(1, std::min<int64_t>(4, rL / 128));  // >= 4 warps per CTA
-    const int slab_t = (int)((rL + 32LL * slab_vs - 1) / (32LL * slab_vs)) * 32;
-    const int slab_minb = slab_t <= 256 ? 2 : 1;
-    const int64_t stage_bytes = 8 * (rL + 2LL * slab_g + ((rL + 1) & ~1LL));
-    const int64_t budget = slab_minb == 2 ? 110 * 1024 : 200 * 1024;
-    int slab_s = (int)std::min<int64_t>(8, budget / stage_bytes);
+    const int slab_t = (int)std::min<int64_t>(256, (rL + 32LL * slab_vs - 1) / (32LL * slab_vs) * 32);
+    const int64_t slab_tw = (int64_t)slab_t * slab_vs;
+    const int64_t slab_ntile = (rL + slab_tw - 1) / slab_tw;
+    int slab_minb = 2;
+    const int64_t stage_bytes = 8 * (2 * slab_tw + 2LL * slab_g);
+    int slab_s = (int)std::min<int64_t>(8, (110 * 1024) / stage_bytes);
+    if (slab_s < 2 * slab_h + 2) {  // one CTA per SM with twice the shared memory
+        slab_minb = 1;
+        slab_s = (int)std::min<int64_t>(8, (200 * 1024) / stage_bytes);
+    }
     slab_s = std::min(slab_s, env_or("CUFSP_KRON_SLAB_S", slab_s));
     if (slab_s < 2 * slab_h + 2) slab = false;
+    {
+        const int64_t resident = (int64_t)device_info().sm_count * slab_minb;
+        const int64_t nseg = std::max<int64_t>(1, std::min<int64_t>(resident / slab_ntile, n_rows / 8));
+        if (slab_ntile * nseg < device_info().sm_count) slab = false;  // too few CTAs to fill the GPU
+    }
     kd->slab_smem = slab ? (size_t)slab_s * (size_t)stage_bytes : 0;
     kd->slab_threads = slab_t;
     std::ostringstream o;
@@ -665,7 +675,7 @@ static void kron_build_rtc(const ModelHost &m, KronData *kd) {
         kd->rows_forward = kd->rows_transpose = false;
         return;
     }
-    // Slab kernels: one CTA per row segment, as many segments as CTAs fit, at least 8 rows each.
+    // Slab kernels: every tile of a row in each of as many row segments as CTAs fit (8 rows at least).
     kd->slab_grid = 0;
     if (slab) {
         int socc = 0;
@@ -676,7 +686,9 @@ static void kron_build_rtc(const ModelHost &m, KronData *kd) {
         if (sok && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&socc, (const void *)mod->kernels[6], slab_t,
                                                                  kd->slab_smem) == cudaSuccess &&
             socc >= 1 && (kd->h_err || (kd->h_err = watch_word_alloc(&kd->d_err)))) {
-            kd->slab_grid = (int)std::min<int64_t>((int64_t)device_info().sm_count * std::min(socc, 8), n_rows / 8);
+            const int64_t resident = (int64_t)device_info().sm_count * std::min(socc, 8);
+            const int64_t nseg = std::max<int64_t>(1, std::min<int64_t>(resident / slab_ntile, n_rows / 8));
+            kd->slab_grid = (int)(slab_ntile * nseg);
         }
         cudaGetLastError();
     }

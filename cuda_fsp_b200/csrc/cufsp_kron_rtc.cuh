@@ -586,8 +586,10 @@ constexpr int VS = CUFSP_KRON_SLAB_VS;  // positions per thread, ST apart
 constexpr int SS = CUFSP_KRON_SLAB_S;   // ring stages
 constexpr int HB = CUFSP_KRON_SLAB_H;   // row halo on each side
 constexpr int GD = CUFSP_KRON_SLAB_G;   // zero guard doubles on each side of a staged x row (even)
-constexpr int PITCH = (int)LEN + 2 * GD;
-constexpr int SD = PITCH + (int)((LEN + 1) & ~1LL);  // stage: guarded x row, then the y row
+constexpr int TW = ST * VS;                          // positions of a CTA's tile of a row
+constexpr long long NTILE = (LEN + TW - 1) / TW;     // tiles per row
+constexpr int PITCH = TW + 2 * GD;
+constexpr int SD = PITCH + TW;                       // stage: guarded x tile, then the y tile
 constexpr long long QN = N / LEN;                    // rows in the box
 #ifndef CUFSP_KRON_SLAB_WAIT_TRIES
 #define CUFSP_KRON_SLAB_WAIT_TRIES (1 << 20)
@@ -670,7 +672,7 @@ __device__ __forceinline__ constexpr int xor_mask(int R) {
 // acc += sum over terms of A_T(p) G_T(q) x[source]; rowp[k] is the staged x row of row q - HB + k.
 template <int T, bool TRANS>
 __device__ __forceinline__ void slab_terms(const double *const (&rowp)[2 * HB + 1], const PosRegs<VS> &g,
-                                           const double (&G)[NR], const int (&pos)[VS], const double (&xv)[VS],
+                                           const double (&G)[NR], const int (&lp)[VS], const double (&xv)[VS],
                                            double (&acc)[VS]) {
     if constexpr (T < NT) {
         constexpr int R = term_rep(T);
@@ -680,14 +682,14 @@ __device__ __forceinline__ void slab_terms(const double *const (&rowp)[2 * HB + 
         const double *src = rowp[HB - DQ] + (GD - DP);
 #pragma unroll
         for (int v = 0; v < VS; ++v) {
-            const double xs = XM ? __shfl_xor_sync(0xffffffffu, xv[v], XM) : src[pos[v]];
+            const double xs = XM ? __shfl_xor_sync(0xffffffffu, xv[v], XM) : src[lp[v]];
             if constexpr (outer_src_one(R)) {
                 acc[v] = fma(g.A[v][T], xs, acc[v]);
             } else {
                 acc[v] = fma(g.A[v][T] * G[R], xs, acc[v]);
             }
         }
-        slab_terms<T + 1, TRANS>(rowp, g, G, pos, xv, acc);
+        slab_terms<T + 1, TRANS>(rowp, g, G, lp, xv, acc);
     }
 }
 
@@ -698,10 +700,16 @@ __device__ __forceinline__ void kron_slab(const CufspKronRtcArgs &a, const doubl
     __shared__ __align__(8) unsigned long long bars[SS];
     __shared__ int failed;
     if (a.d_skip && *a.d_skip) return;
+    // CTA = (tile of TW positions, segment of rows); the grid is a multiple of NTILE.
     const long long nrows = a.q_end - a.q_begin;
-    const long long seg = (nrows + gridDim.x - 1) / gridDim.x;
-    const long long q0 = a.q_begin + (long long)blockIdx.x * seg;
+    const long long nseg = gridDim.x / NTILE;
+    const long long tile = blockIdx.x % NTILE, segi = blockIdx.x / NTILE;
+    const long long seg = (nrows + nseg - 1) / nseg;
+    const long long q0 = a.q_begin + segi * seg;
     const long long q1 = min(a.q_end, q0 + seg);
+    const long long p0 = tile * TW;                           // first position of the tile
+    const long long xlo = max(0LL, p0 - GD), xhi = min(LEN, p0 + TW + GD);  // staged x positions
+    const long long ylen = min(LEN, p0 + TW) - p0;
     if (q0 >= q1) return;  // whole CTA leaves before any barrier or copy
     const int tid = threadIdx.x;
     for (int k = tid; k < SS * SD; k += ST) smem[k] = 0.0;  // guards and never-copied rows stay zero
@@ -725,9 +733,9 @@ __device__ __forceinline__ void kron_slab(const CufspKronRtcArgs &a, const doubl
         }
         const bool own = ACCUM && p >= q0 && p < q1;
         double *st = stage(p);
-        mbar_expect_tx(bar(p), (unsigned)(LEN * 8 * (own ? 2 : 1)));
-        tma_load(st + GD, x + p * LEN, (unsigned)(LEN * 8), bar(p));
-        if (own) tma_load(st + PITCH, y + p * LEN, (unsigned)(LEN * 8), bar(p));
+        mbar_expect_tx(bar(p), (unsigned)(8 * ((xhi - xlo) + (own ? ylen : 0))));
+        tma_load(st + (xlo - p0 + GD), x + p * LEN + xlo, (unsigned)(8 * (xhi - xlo)), bar(p));
+        if (own) tma_load(st + PITCH, y + p * LEN + p0, (unsigned)(8 * ylen), bar(p));
     };
     long long issued = pbase - 1;
     if (tid == 0) {
@@ -740,17 +748,17 @@ __device__ __forceinline__ void kron_slab(const CufspKronRtcArgs &a, const doubl
     const double *__restrict__ tab = a.tables;
     const double alpha = a.d_alpha ? __ldg(a.d_alpha) : 1.0;
     PosRegs<VS> g;
-    int pos[VS];
+    int pos[VS], lp[VS];
     bool act[VS];
 #pragma unroll
     for (int v = 0; v < VS; ++v) {
-        pos[v] = v * ST + tid;
+        pos[v] = (int)p0 + v * ST + tid;
         act[v] = pos[v] < LEN;
         int xi[KI];
         inner_decode(act[v] ? pos[v] : LEN - 1, xi);
         g.D0[v] = 0.0;
         chunk_prologue<0, TRANS, VS>(a, alpha, tab, xi, v, g);
-        if (!act[v]) pos[v] = 0;  // idle position: reads stay inside the row, nothing is written
+        lp[v] = v * ST + tid;  // index in the staged tile; an idle position reads, writes nothing
     }
 
     bool ok = true;
@@ -773,21 +781,21 @@ __device__ __forceinline__ void kron_slab(const CufspKronRtcArgs &a, const doubl
 #pragma unroll
             for (int k = 0; k <= 2 * HB; ++k) rowp[k] = stage(q - HB + k);
             const double *xs = rowp[HB] + GD;
-            const double *ys = rowp[HB] + PITCH;
+            const double *ys = rowp[HB] + PITCH;  // y tile: index lp
             double xv[VS], acc[VS], dg[VS];
 #pragma unroll
             for (int v = 0; v < VS; ++v) {
-                xv[v] = xs[pos[v]];
+                xv[v] = xs[lp[v]];
                 acc[v] = 0.0;
                 dg[v] = g.D0[v];
             }
-            slab_terms<0, TRANS>(rowp, g, G, pos, xv, acc);
+            slab_terms<0, TRANS>(rowp, g, G, lp, xv, acc);
             rows_diag<0, VS>(g, Gd, dg);
 #pragma unroll
             for (int v = 0; v < VS; ++v) {
                 if (act[v]) {
                     double r = fma(-dg[v], xv[v], acc[v]);
-                    if (ACCUM) r += ys[pos[v]];
+                    if (ACCUM) r += ys[lp[v]];
                     __stcs(y + q * LEN + pos[v], r);
                 }
             }

@@ -200,3 +200,27 @@ def test_slab_watchdog(cuda, monkeypatch):
     assert A.watchdog() == 1
     assert A.watchdog() == 0
     check_rows(m)  # a normal generator of the same network
+
+
+@pytest.mark.parametrize("case", ["gene_rows_of_4096", "three_species_change_of_2", "three_species_plane"])
+def test_tiled_slab_kernels_match_oracle(cuda, case, monkeypatch):
+    """Rows longer than a CTA's tile (1024 positions): the slab kernels split every row into tiles,
+    each staged with guards of up to 512 positions for its inner neighbours.  A 2.1M-state gene box
+    (rows of 4096 positions, forward and transposed through tiles), a 3-species network with a change
+    of 2 molecules (rows of 16,384 positions, neighbours 256 positions away), and the plane-shaped
+    3-species network, whose transposed action goes through the tiled slab kernel."""
+    monkeypatch.delenv("CUFSP_KRON_ROWS", raising=False)
+    if case == "gene_rows_of_4096":
+        m = models.gene_expression((1, 1, 1, 511, 511), time_varying=False)
+    elif case == "three_species_change_of_2":
+        m = models.mass_action_3(bounds=(127, 127, 127))
+        m.nu[0] = (2, 0, 0)
+        m.nu[6] = (0, -2, 1)
+    else:
+        m = models.mass_action_3(bounds=(127, 127, 127))
+    A = check_rows(m)
+    if case == "three_species_plane":
+        assert "plane kernel" in A.describe(), A.describe()
+    else:
+        assert "slab kernel" in A.describe(), A.describe()
+    assert A.watchdog() == 0
