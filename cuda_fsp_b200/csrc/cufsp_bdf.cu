@@ -20,7 +20,9 @@
 // streaming kernel with a deterministic reduction; the host keeps the step-control scalars and
 // reads back one small block per GMRES iteration.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -162,6 +164,8 @@ struct cufsp_bdf_s {
     double *V = nullptr;  // maxl + 1 vectors
     double *w = nullptr, *ypred = nullptr, *d = nullptr, *tmp = nullptr;
     double *d_scal = nullptr, *h_scal = nullptr;
+    unsigned *h_seq = nullptr;  // sequence word of the scalar block (pinned host memory)
+    unsigned seq = 0;
     ReduceScratch rs;
     double gam[kMaxOrder + 2] = {}, econst[kMaxOrder + 2] = {};
     // state
@@ -193,10 +197,48 @@ cufsp_status apply(cufsp_bdf *B, double t, double alpha, const double *x, bool a
     return mat_apply(B->A, B->cbuf.data(), alpha, nullptr, nullptr, x, accumulate, y, st);
 }
 
+// Copies scalars [first, first + count) of the device block into the pinned host block (reachable
+// from the device through unified addressing), then raises the sequence word.
+__global__ void k_publish(const double *__restrict__ d, double *h, int first, int count, unsigned *h_seq,
+                          unsigned seq) {
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < count; ++k) h[first + k] = d[first + k];
+        __threadfence_system();
+        *(volatile unsigned *)h_seq = seq;
+    }
+}
+
+bool spin_fetch() {  // CUFSP_BDF_SPIN=0: a copy command and a stream synchronisation instead
+    static const bool on = [] {
+        const char *e = getenv("CUFSP_BDF_SPIN");
+        return !e || atoi(e) != 0;
+    }();
+    return on;
+}
+
+// The host reads the scalars the step control needs, once per GMRES iteration and a few times per
+// step.  The scalars travel by k_publish and the host waits on the sequence word, which saves the copy
+// command and the synchronisation call of each round trip.  The wait is bounded: the stream is
+// queried every 1024 polls, and a finished or failed stream, or 10 s, ends it; a synchronisation then
+// returns any error.
 cufsp_status fetch(cufsp_bdf *B, int first, int count, cudaStream_t st) {
-    CUFSP_CUDA_TRY(cudaMemcpyAsync(B->h_scal + first, B->d_scal + first, sizeof(double) * count,
-                                   cudaMemcpyDeviceToHost, st));
-    CUFSP_CUDA_TRY(cudaStreamSynchronize(st));
+    if (!spin_fetch()) {
+        CUFSP_CUDA_TRY(cudaMemcpyAsync(B->h_scal + first, B->d_scal + first, sizeof(double) * count,
+                                       cudaMemcpyDeviceToHost, st));
+        CUFSP_CUDA_TRY(cudaStreamSynchronize(st));
+        return mat_check_watchdog(B->A, "cufsp_bdf_advance");
+    }
+    const unsigned seq = ++B->seq;
+    k_publish<<<1, 32, 0, st>>>(B->d_scal, B->h_scal, first, count, B->h_seq, seq);
+    CUFSP_CUDA_TRY(cudaGetLastError());
+    const auto t0 = std::chrono::steady_clock::now();
+    for (unsigned it = 1; *(volatile unsigned *)B->h_seq != seq; ++it) {
+        if ((it & 1023) == 0) {
+            if (cudaStreamQuery(st) != cudaErrorNotReady) break;
+            if (std::chrono::steady_clock::now() - t0 > std::chrono::seconds(10)) break;
+        }
+    }
+    if (*(volatile unsigned *)B->h_seq != seq) CUFSP_CUDA_TRY(cudaStreamSynchronize(st));
     return mat_check_watchdog(B->A, "cufsp_bdf_advance");
 }
 
@@ -418,7 +460,9 @@ void release(cufsp_bdf *B) {
     if (B->store) cudaFree(B->store);
     if (B->d_scal) cudaFree(B->d_scal);
     if (B->h_scal) cudaFreeHost(B->h_scal);
+    if (B->h_seq) cudaFreeHost(B->h_seq);
     B->store = B->d_scal = B->h_scal = nullptr;
+    B->h_seq = nullptr;
     B->rs.release();
 }
 
@@ -452,10 +496,12 @@ extern "C" cufsp_status cufsp_bdf_create(cufsp_mat *A, const double *coefs, doub
     cufsp_status s = CUFSP_SUCCESS;
     if (dev_malloc(&B->store, sizeof(double) * B->ld * nvec) != cudaSuccess ||
         dev_malloc(&B->d_scal, sizeof(double) * kNScal) != cudaSuccess ||
-        cudaMallocHost(&B->h_scal, sizeof(double) * kNScal) != cudaSuccess) {
+        cudaMallocHost(&B->h_scal, sizeof(double) * kNScal) != cudaSuccess ||
+        cudaMallocHost(&B->h_seq, 64) != cudaSuccess) {
         cudaGetLastError();
         s = set_error(CUFSP_ERR_ALLOC, "cufsp_bdf_create: device allocation failed");
     }
+    if (s == CUFSP_SUCCESS) *(volatile unsigned *)B->h_seq = 0u;
     if (s == CUFSP_SUCCESS) s = B->rs.init(device_info().sm_count * 4, 64);
     if (s != CUFSP_SUCCESS) {
         release(B);
