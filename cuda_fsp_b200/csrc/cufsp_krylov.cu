@@ -18,6 +18,7 @@
 // Deviations from the reference: k1 is reset every step (reference defect: KryExpvFSP.h:61), pi is
 // exact (:48), a zero vector is returned unchanged, NaN/Inf and exhausted limits return errors.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -399,6 +400,79 @@ cufsp_status arnoldi_launches(cufsp_expv *E, double *v, cudaStream_t st, bool wi
     return CUFSP_SUCCESS;
 }
 
+// The state block travels to the host once per pass: a one-CTA kernel copies it into pinned host
+// memory (reachable from the device through unified addressing) and raises a sequence word that the
+// host polls, instead of a copy command and a stream synchronisation.  The poll is bounded: the
+// stream is queried every 1024 polls, and a finished or failed stream, or 10 s, ends it; a
+// synchronisation then returns any error.  The pinned buffer is per host thread (calls are
+// synchronous, so one buffer serves every driver of the thread).  CUFSP_KRYLOV_SPIN=0: a copy and a
+// synchronisation.
+__global__ void k_publish_state(const double *__restrict__ d, double *h, int words, unsigned *h_seq, unsigned seq) {
+    for (int k = threadIdx.x; k < words; k += blockDim.x) h[k] = d[k];
+    __threadfence_system();
+    __syncthreads();
+    if (threadIdx.x == 0) *(volatile unsigned *)h_seq = seq;
+}
+
+struct PinnedState {
+    double *p = nullptr;
+    unsigned *seq = nullptr;
+    size_t bytes = 0;
+    unsigned n = 0;
+    ~PinnedState() {
+        if (p) cudaFreeHost(p);
+        if (seq) cudaFreeHost(seq);
+    }
+};
+thread_local PinnedState tl_pin;
+
+bool spin_state() {
+    static const bool on = [] {
+        const char *e = getenv("CUFSP_KRYLOV_SPIN");
+        return !e || atoi(e) != 0;
+    }();
+    return on;
+}
+
+cufsp_status fetch_state(cufsp_expv *E, cudaStream_t st) {
+    bool spin = spin_state();
+    if (spin && tl_pin.bytes < E->state_bytes) {
+        if (tl_pin.p) cudaFreeHost(tl_pin.p);
+        tl_pin.p = nullptr;
+        tl_pin.bytes = 0;
+        if (!tl_pin.seq && cudaHostAlloc((void **)&tl_pin.seq, 64, cudaHostAllocPortable | cudaHostAllocMapped) != cudaSuccess)
+            tl_pin.seq = nullptr;
+        if (tl_pin.seq &&
+            cudaHostAlloc((void **)&tl_pin.p, E->state_bytes, cudaHostAllocPortable | cudaHostAllocMapped) == cudaSuccess) {
+            tl_pin.bytes = E->state_bytes;
+            *(volatile unsigned *)tl_pin.seq = tl_pin.n;
+        } else {
+            cudaGetLastError();
+            tl_pin.p = nullptr;
+            spin = false;
+        }
+    }
+    if (!spin) {
+        CUFSP_CUDA_TRY(cudaMemcpyAsync(E->hstate.data(), E->d_state, E->state_bytes, cudaMemcpyDeviceToHost, st));
+        CUFSP_CUDA_TRY(cudaStreamSynchronize(st));
+        return CUFSP_SUCCESS;
+    }
+    const unsigned seq = ++tl_pin.n;
+    const int words = (int)(E->state_bytes / sizeof(double));
+    k_publish_state<<<1, 256, 0, st>>>(E->d_state, tl_pin.p, words, tl_pin.seq, seq);
+    CUFSP_CUDA_TRY(cudaGetLastError());
+    const auto t0 = std::chrono::steady_clock::now();
+    for (unsigned it = 1; *(volatile unsigned *)tl_pin.seq != seq; ++it) {
+        if ((it & 1023) == 0) {
+            if (cudaStreamQuery(st) != cudaErrorNotReady) break;
+            if (std::chrono::steady_clock::now() - t0 > std::chrono::seconds(10)) break;
+        }
+    }
+    if (*(volatile unsigned *)tl_pin.seq != seq) CUFSP_CUDA_TRY(cudaStreamSynchronize(st));
+    std::memcpy(E->hstate.data(), tl_pin.p, E->state_bytes);
+    return CUFSP_SUCCESS;
+}
+
 bool graphs_enabled() {
     static const bool on = [] {
         const char *e = getenv("CUFSP_KRYLOV_GRAPH");
@@ -460,8 +534,8 @@ cufsp_status arnoldi_pass(cufsp_expv *E, double *v, cudaStream_t st, bool with_a
         if (s != CUFSP_SUCCESS) return s;
     }
     const int m = E->m;
-    CUFSP_CUDA_TRY(cudaMemcpyAsync(E->hstate.data(), E->d_state, E->state_bytes, cudaMemcpyDeviceToHost, st));
-    CUFSP_CUDA_TRY(cudaStreamSynchronize(st));
+    s = fetch_state(E, st);
+    if (s != CUFSP_SUCCESS) return s;
     // basis data for the adjoint (leading mb x mb block of H, rho, beta)
     const int mp2 = m + 2;
     const double *hH = E->hstate.data();
