@@ -203,7 +203,7 @@ struct cufsp_mat_s {
     std::vector<double> coef_buf;
     // host-buffer pipeline resources (created on first use)
     double *d_x = nullptr, *d_y = nullptr;
-    cudaStream_t s_in = nullptr, s_in2 = nullptr, s_comp = nullptr, s_out = nullptr;
+    cudaStream_t s_in = nullptr, s_comp = nullptr, s_out = nullptr;
     std::vector<cudaEvent_t> ev;
 };
 

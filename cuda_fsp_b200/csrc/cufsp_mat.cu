@@ -119,7 +119,6 @@ extern "C" cufsp_status cufsp_mat_destroy(cufsp_mat *A) {
     if (A->d_y) cudaFree(A->d_y);
     for (cudaEvent_t e : A->ev) cudaEventDestroy(e);
     if (A->s_in) cudaStreamDestroy(A->s_in);
-    if (A->s_in2) cudaStreamDestroy(A->s_in2);
     if (A->s_comp) cudaStreamDestroy(A->s_comp);
     if (A->s_out) cudaStreamDestroy(A->s_out);
     delete A;
@@ -215,7 +214,6 @@ extern "C" cufsp_status cufsp_mat_action_host(cufsp_mat *A, double t, const doub
         CUFSP_CUDA_TRY(dev_malloc(&A->d_x, sizeof(double) * n));
         CUFSP_CUDA_TRY(dev_malloc(&A->d_y, sizeof(double) * n));
         CUFSP_CUDA_TRY(cudaStreamCreateWithFlags(&A->s_in, cudaStreamNonBlocking));
-        CUFSP_CUDA_TRY(cudaStreamCreateWithFlags(&A->s_in2, cudaStreamNonBlocking));
         CUFSP_CUDA_TRY(cudaStreamCreateWithFlags(&A->s_comp, cudaStreamNonBlocking));
         CUFSP_CUDA_TRY(cudaStreamCreateWithFlags(&A->s_out, cudaStreamNonBlocking));
         A->ev.resize(3 * kSlabs);
@@ -227,12 +225,8 @@ extern "C" cufsp_status cufsp_mat_action_host(cufsp_mat *A, double t, const doub
     std::vector<int64_t> b(kSlabs + 1);
     for (int k = 0; k <= kSlabs; ++k) b[k] = (rows * k / kSlabs) * gran;
     cudaEvent_t *evx = A->ev.data(), *evy = evx + kSlabs, *evc = evy + kSlabs;
-    // y slabs on a second input stream when CUFSP_HOST_IN_STREAMS=2 (two copy engines for host->device)
-    static const bool two_in = [] {
-        const char *e = getenv("CUFSP_HOST_IN_STREAMS");
-        return e && atoi(e) == 2;
-    }();
-    cudaStream_t ys = two_in ? A->s_in2 : A->s_in;
+    // One host->device stream: a second one for the y slabs moved the same 71 GB/s (the PCIe link).
+    cudaStream_t ys = A->s_in;
     for (int k = 0; k < kSlabs; ++k) {
         const int64_t cnt = b[k + 1] - b[k];
         if (cnt > 0) {
