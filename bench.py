@@ -676,7 +676,9 @@ def run_leg(args):
     """One leg alone, for profiling its kernels under ncu (small steps, one JSON line, no extras):
       sparse  the CSR/HYB generator action y += A x on mass_action_3 (--box, default 255^3)
       kgen    the KRONECKER action of the 5-species gene network (--box, default 1,1,1,127,8191): the
-              specialised general kernel
+              slab kernel
+      kslab3  forward and transposed KRONECKER actions of the 3-species network with two reactions
+              moving 2 molecules (--box, default 255^3): the tiled slab kernels
       krylov  Krylov steps exp(tA)p0 on mass_action_3 (--box; above 2^20 states the launch sequence
               of plane-kernel matvecs and the k_mdot / k_mupd / k_comb vector kernels)
       adjoint one log-likelihood gradient on the gene model (--box, default 1,1,1,127,127)
@@ -729,6 +731,37 @@ def run_leg(args):
         ms = ev0.elapsed_time(ev1) / args.steps
         out.update({"n_states": m.n_states, "us_per_action": round(ms * 1e3, 2),
                     "gbs": round(BYTES_PER_STATE * m.n_states / (ms * 1e-3) / 1e9, 1), "kernel": A.describe()})
+    elif args.leg == "kslab3":
+        # the 3-species network with reactions 0 and 6 moving 2 molecules (outside the plane kernel's
+        # shape): forward y += A x and transposed y = A^T x through the slab kernels
+        m = models.mass_action_3(bounds=box) if box else models.mass_action_3()
+        m.nu[0] = (2, 0, 0)
+        m.nu[6] = (0, -2, 1)
+        A = FSPMat.from_model(m, MatrixFormat.KRONECKER)
+        g = torch.Generator(device="cuda").manual_seed(7)
+        xs = [torch.rand(m.n_states, dtype=torch.float64, device="cuda", generator=g) for _ in range(2)]
+        ys = [torch.zeros(m.n_states, dtype=torch.float64, device="cuda") for _ in range(2)]
+        c = m.coefs(0)
+        res = {}
+        for form in ("forward", "transposed"):
+            def act(i):
+                if form == "forward":
+                    A.apply(xs[i % 2], ys[i % 2], coefs=c, beta=1.0)
+                else:
+                    A.apply_transpose(xs[i % 2], ys[i % 2], coefs=c)
+            for i in range(max(3, args.warmup)):
+                act(i)
+            torch.cuda.synchronize()
+            ev0.record()
+            for i in range(args.steps):
+                act(i)
+            ev1.record()
+            torch.cuda.synchronize()
+            ms = ev0.elapsed_time(ev1) / args.steps
+            bps = BYTES_PER_STATE if form == "forward" else 16
+            res[form] = {"us_per_action": round(ms * 1e3, 2), "bytes_per_state": bps,
+                         "gbs": round(bps * m.n_states / (ms * 1e-3) / 1e9, 1)}
+        out.update({"n_states": m.n_states, **res, "kernel": A.describe()})
     elif args.leg == "krylov":
         m = models.mass_action_3(bounds=box) if box else models.mass_action_3()
         A = FSPMat.from_model(m, MatrixFormat.KRONECKER)
@@ -835,7 +868,8 @@ def main():
     ap.add_argument("--sets", type=int, default=4, help="rotating (x, y) input pairs; parameter sets of the gradbatch leg")
     ap.add_argument("--no-extras", action="store_true",
                     help="time the generator action only (no e2e, expmv or CPU legs); for profiling runs")
-    ap.add_argument("--leg", choices=["sparse", "kgen", "krylov", "adjoint", "gradbatch", "bdf", "states", "iopsweep"],
+    ap.add_argument("--leg", choices=["sparse", "kgen", "kslab3", "krylov", "adjoint", "gradbatch", "bdf", "states",
+                                      "iopsweep"],
                     default=None,
                     help="run one leg alone (profiling runs; see run_leg)")
     ap.add_argument("--box", default=None, help="box bounds of the leg, comma separated")
