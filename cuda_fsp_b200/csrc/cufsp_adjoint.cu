@@ -465,7 +465,9 @@ extern "C" cufsp_status cufsp_likelihood_grad(cufsp_mat *A, const double *coefs,
                     }
                     launch_adj_bilinear(ba, red_grid, st);
                     CUFSP_CUDA_TRY(cudaGetLastError());
-                    CUFSP_CUDA_TRY(cudaStreamSynchronize(st));  // d_coef / uh are reused by the next sub-step
+                    // No synchronisation: d_coef, uh and the bases are reused in stream order, and the
+                    // pageable copy above has taken coefm before returning.  (With CUFSP_VERBOSE the
+                    // kernels' time then shows in the next sub-step's "backward steps" phase.)
                     t_kern += since(tp);
                 }
                 b_end = a0;
