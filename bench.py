@@ -439,7 +439,7 @@ def batched_secondary(n_sets: int = 256, sample: int = 4) -> dict:
     p0 = B.pack([mm.p0() for mm in ms])
     p = p0.clone()
     t0 = time.perf_counter()
-    B.solve(30.0, p)  # chooses the launch shape (autotuner) and warms up; untimed
+    B.solve(30.0, p)  # chooses the launch shape (autotuner), captures the graph and warms up; untimed
     tune_s = time.perf_counter() - t0
     p.copy_(p0)
     torch.cuda.synchronize()
@@ -466,7 +466,16 @@ def batched_secondary(n_sets: int = 256, sample: int = 4) -> dict:
             "single_instance_solves_per_s": round(len(idx) / single_s, 3),
             "single_instance_sample": f"{len(idx)} of the same instances through KryExpvFSP",
             "max_1norm_diff_vs_single": max(errs), "steps_mean": float(np.mean([s_["steps"] for s_ in stats])),
-            "launch": B.describe(), "autotune_and_warmup_s": round(tune_s, 1)}
+            "launch": B.describe(), "first_call_s": round(tune_s, 1),
+            "autotune_s": _autotune_seconds(B.describe())}
+
+
+def _autotune_seconds(describe: str):
+    """The autotuner's own wall time (candidate compiles and trial launches), as the solver reports it;
+    None when the launch shape came from the tuning cache or the environment."""
+    import re
+    hit = re.search(r"autotuner ([0-9.]+) s", describe)
+    return float(hit.group(1)) if hit else None
 
 
 def batched_sharded_secondary(world: int, rank: int, dev, per_rank: int = 256) -> dict | None:
@@ -493,13 +502,15 @@ def batched_sharded_secondary(world: int, rank: int, dev, per_rank: int = 256) -
             "s_per_batch": round(dt.item(), 3), "scaling": "weak", "failed": sum(1 for r in res if r["status"] != 0)}
 
 
-def gradient_secondary(n_sets: int = 64, workers: int = 2) -> dict:
+def gradient_secondary(n_sets: int = 64, workers: int = 4, sample: int = 8) -> dict:
     """Gradient leg: d log L / d log theta for the 12 rates of the gene-expression model (131,072 states) from
     1,000 seeded-SSA cells at 8 log-spaced times in [1, 60], (n, c) histograms marginalised over the
     gene states, for n_sets parameter sets (rates within half a decade of nominal) at once
-    (cufsp_likelihood_grad_batched: `workers` concurrent adjoint solves; at this size each solve's
-    Arnoldi passes fill the GPU, so two workers overlap one solve's passes with the other's host-side
-    step control); one single-set gradient and one log-likelihood evaluation are timed beside it."""
+    (cufsp_likelihood_grad_batched: `workers` concurrent adjoint solves, each worker's persistent
+    Arnoldi passes on an equal share of the SMs, so that one solve's passes overlap the others' host-side
+    step control).  The comparator is the same path one set at a time on `sample` of the same sets
+    (every n_sets/sample-th: the sets differ in cost, since the step count follows the rates), whose
+    results the batched ones must match; one log-likelihood evaluation is timed beside it."""
     import torch
     from cuda_fsp_b200 import Likelihood, generate_data, histograms, models
     m = models.gene_expression((1, 1, 1, 127, 127), time_varying=False)
@@ -511,14 +522,19 @@ def gradient_secondary(n_sets: int = 64, workers: int = 2) -> dict:
     sets = np.stack([m.coefs(0) * 10.0 ** rng.uniform(-0.5, 0.5, m.nr) for _ in range(n_sets)])
     L.gradient(sets[0])  # warm-up (kernel compilation, graphs)
     torch.cuda.synchronize()
+    idx = [i * n_sets // sample for i in range(sample)]
+    single, ref = 0.0, []
+    for i in idx:
+        t0 = time.perf_counter()
+        ref.append(L.gradient(sets[i]))
+        torch.cuda.synchronize()
+        single += time.perf_counter() - t0
     t0 = time.perf_counter()
-    L.gradient(sets[1])
-    torch.cuda.synchronize()
-    single = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    L.gradient_batched(sets, workers=workers)
+    ll_b, g_b = L.gradient_batched(sets, workers=workers)
     torch.cuda.synchronize()
     batched = time.perf_counter() - t0
+    diff = max(float(np.abs(g_b[i] - g).max() / max(np.abs(g).max(), 1e-300)) for i, (_, g) in zip(idx, ref))
+    dll = max(abs(ll_b[i] - l) / abs(l) for i, (l, _) in zip(idx, ref))
     t0 = time.perf_counter()
     L.evaluate(sets[0])
     torch.cuda.synchronize()
@@ -526,7 +542,9 @@ def gradient_secondary(n_sets: int = 64, workers: int = 2) -> dict:
     return {"metric": "grad logL grads/s", "workload": "gene_expression 131,072 states, 12 rates, 8 times in [1, 60], "
             f"1,000 SSA cells per time, marginalised over gene states, {n_sets} parameter sets",
             "value": round(n_sets / batched, 3), "s_per_batch": round(batched, 3), "workers": workers,
-            "single_gradient_s": round(single, 3), "single_grads_per_s": round(1.0 / single, 3),
+            "single_grads_per_s": round(len(idx) / single, 3),
+            "single_sample": f"{len(idx)} of the same sets one at a time (cufsp_likelihood_grad)",
+            "max_rel_diff_grad_vs_single": diff, "max_rel_diff_logL_vs_single": dll,
             "s_per_loglik": round(ev, 3)}
 
 

@@ -12,18 +12,21 @@
 #include <sys/stat.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <functional>
+#include <iomanip>
 #include <map>
 #include <memory>
 #include <mutex>
 #include <numeric>
 #include <sstream>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "cufsp_internal.h"
@@ -54,14 +57,13 @@ int env_int(const char *name, int dflt) {
     return v ? atoi(v) : dflt;
 }
 
-std::shared_ptr<BatchKernel> batch_kernel(const std::string &src, std::string &why) {
-    std::lock_guard<std::mutex> lock(g_batch_mu);
-    auto it = g_batch_cache.find(src);
-    if (it != g_batch_cache.end()) return it->second;
+// NVRTC compile of one batched-kernel source to a cubin (no lock: NVRTC programs are independent, so
+// the autotuner compiles its candidate sources on parallel host threads).
+bool compile_cubin(const std::string &src, std::vector<char> &cubin, std::string &why) {
     nvrtcProgram prog;
     if (nvrtcCreateProgram(&prog, src.c_str(), "cufsp_batch.cu", 0, nullptr, nullptr) != NVRTC_SUCCESS) {
         why = "nvrtcCreateProgram failed";
-        return nullptr;
+        return false;
     }
     const char *opts[] = {"--gpu-architecture=sm_100a", "-std=c++17", "--fmad=true", "-lineinfo",
                           "-I/usr/local/cuda/include"};
@@ -73,10 +75,10 @@ std::shared_ptr<BatchKernel> batch_kernel(const std::string &src, std::string &w
         if (ls > 1) nvrtcGetProgramLog(prog, &log[0]);
         why = std::string("NVRTC: ") + nvrtcGetErrorString(rc) + ": " + log.substr(0, 3000);
         nvrtcDestroyProgram(&prog);
-        return nullptr;
+        return false;
     }
     size_t cs = 0;
-    std::vector<char> cubin;
+    cubin.clear();
     if (nvrtcGetCUBINSize(prog, &cs) == NVRTC_SUCCESS && cs > 0) {
         cubin.resize(cs);
         if (nvrtcGetCUBIN(prog, cubin.data()) != NVRTC_SUCCESS) cubin.clear();
@@ -84,8 +86,16 @@ std::shared_ptr<BatchKernel> batch_kernel(const std::string &src, std::string &w
     nvrtcDestroyProgram(&prog);
     if (cubin.empty()) {
         why = "NVRTC produced no cubin";
-        return nullptr;
+        return false;
     }
+    return true;
+}
+
+// Loads a compiled cubin into the process-wide kernel cache (caller holds g_batch_mu).
+std::shared_ptr<BatchKernel> load_kernel_locked(const std::string &src, const std::vector<char> &cubin,
+                                                std::string &why) {
+    auto it = g_batch_cache.find(src);
+    if (it != g_batch_cache.end()) return it->second;
     auto bk = std::make_shared<BatchKernel>();
     cudaError_t e = cudaLibraryLoadData(&bk->lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0);
     if (e == cudaSuccess) e = cudaLibraryGetKernel(&bk->k, bk->lib, "cufsp_batch_expv");
@@ -103,6 +113,36 @@ std::shared_ptr<BatchKernel> batch_kernel(const std::string &src, std::string &w
     }
     g_batch_cache[src] = bk;
     return bk;
+}
+
+std::shared_ptr<BatchKernel> batch_kernel(const std::string &src, std::string &why) {
+    std::lock_guard<std::mutex> lock(g_batch_mu);
+    auto it = g_batch_cache.find(src);
+    if (it != g_batch_cache.end()) return it->second;
+    std::vector<char> cubin;
+    if (!compile_cubin(src, cubin, why)) return nullptr;
+    return load_kernel_locked(src, cubin, why);
+}
+
+// Compiles the sources not yet in the kernel cache on one host thread each and loads them.
+void prefetch_kernels(const std::vector<std::string> &srcs) {
+    std::vector<std::string> todo;
+    {
+        std::lock_guard<std::mutex> lock(g_batch_mu);
+        for (const std::string &s : srcs)
+            if (!g_batch_cache.count(s) && std::find(todo.begin(), todo.end(), s) == todo.end()) todo.push_back(s);
+    }
+    if (todo.size() < 2) return;  // nothing to overlap; batch_kernel compiles on demand
+    std::vector<std::vector<char>> cubins(todo.size());
+    std::vector<std::string> why(todo.size());
+    std::vector<char> ok(todo.size(), 0);
+    std::vector<std::thread> th;
+    for (size_t i = 0; i < todo.size(); ++i)
+        th.emplace_back([&, i] { ok[i] = compile_cubin(todo[i], cubins[i], why[i]); });
+    for (auto &t : th) t.join();
+    std::lock_guard<std::mutex> lock(g_batch_mu);
+    for (size_t i = 0; i < todo.size(); ++i)
+        if (ok[i]) load_kernel_locked(todo[i], cubins[i], why[i]);  // failures recompile (and report) on demand
 }
 
 void emit_fn2(std::ostringstream &s, const char *name, const std::vector<int> &v, int ns) {
@@ -181,6 +221,8 @@ struct cufsp_batch_s {
     std::shared_ptr<BatchKernel> kern;
     int n_clusters = 0;
     double tuned_ms = 0.0;
+    double tune_s = 0.0;                   // wall time of the autotuner (compiles and trial launches)
+    double tune_compile_s = 0.0;           // of which compiling the candidate shapes
     bool tuned = false;
     // graph of the last solve
     cudaGraphExec_t gexec = nullptr;
@@ -272,6 +314,9 @@ std::string describe_shape(const cufsp_batch *B) {
     d << "batched Krylov (NVRTC, sm_100a, one persistent launch): " << B->n_inst << " instances, m=" << B->m
       << (B->iop ? " IOP" : "") << ", " << B->n_clusters << " clusters x " << B->cluster << " CTAs x " << B->threads
       << " threads (" << B->minb << " CTA/SM bound), smem " << B->kern->smem << " B/CTA";
+    if (B->tune_s > 0.0)
+        d << "; autotuner " << std::fixed << std::setprecision(1) << B->tune_s << " s on " << B->n_sample
+          << " instances (compiles " << B->tune_compile_s << " s)";
     return d.str();
 }
 
@@ -308,6 +353,13 @@ cufsp_status autotune(cufsp_batch *B, double t_final, const double *p, cudaStrea
     } else {
         const Shape cands[] = {{8, 256, 1}, {16, 256, 1}, {4, 512, 1}, {8, 512, 1},
                                {16, 512, 1}, {8, 256, 2}, {16, 256, 2}};
+        const auto t_tune = std::chrono::steady_clock::now();
+        {
+            std::vector<std::string> srcs;
+            for (const Shape &cd : cands) srcs.push_back(shape_source(B, cd.threads, cd.minb));
+            prefetch_kernels(srcs);
+        }
+        B->tune_compile_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_tune).count();
         const int64_t total = B->offsets.back();
         if (!B->d_scratch) CUFSP_CUDA_TRY(dev_malloc(&B->d_scratch, sizeof(double) * (size_t)total));
         double best = 1e300;
@@ -342,6 +394,7 @@ cufsp_status autotune(cufsp_batch *B, double t_final, const double *p, cudaStrea
         cudaEventDestroy(e1);
         if (B->cluster == 0) return set_error(CUFSP_ERR_CUDA, "batched solver: no launch shape fits this device: " + why);
         B->tuned_ms = best;
+        B->tune_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_tune).count();
         cache_store(key, Shape{B->cluster, B->threads, B->minb}, best);
     }
     B->kern = batch_kernel(shape_source(B, B->threads, B->minb), why);
