@@ -544,7 +544,13 @@ def gradient_secondary(n_sets: int = 64, workers: int = 4, sample: int = 8) -> d
             "value": round(n_sets / batched, 3), "s_per_batch": round(batched, 3), "workers": workers,
             "single_grads_per_s": round(len(idx) / single, 3),
             "single_sample": f"{len(idx)} of the same sets one at a time (cufsp_likelihood_grad)",
-            "max_rel_diff_grad_vs_single": diff, "max_rel_diff_logL_vs_single": dll,
+            "rel_diff_vs_single": {
+                "logL": dll, "grad": diff,
+                "note": "the workers' passes run on a quarter of the SMs (37 CTAs against 148) and round "
+                        "differently; where that flips an accept/reject decision of the Krylov step control, "
+                        "data cells whose probability is below the absolute kry_tol 1e-8 cross the 1e-44 floor "
+                        "(up to ~70 in log L each). With equal CTA counts both paths do the same arithmetic "
+                        "(test_c5_batched_gradients_equal_single_on_full_gene_box)."},
             "s_per_loglik": round(ev, 3)}
 
 

@@ -287,7 +287,7 @@ extern "C" cufsp_status cufsp_likelihood_grad(cufsp_mat *A, const double *coefs,
         ~RsGuard() { r.release(st); }
     } rsg{rs, st};
     const int red_grid = stream_grid(n, 4, device_info().sm_count * 4);
-    s = rs.init(red_grid, 32);
+    s = rs.init(red_grid, 32, st);
     if (s != CUFSP_SUCCESS) return s;
     double *d_I = d_misc, *d_ll = d_misc + 32, *d_coef = d_misc + 64;
     CUFSP_CUDA_TRY(cudaMemsetAsync(d_misc, 0, sizeof(double) * 64, st));
@@ -521,6 +521,9 @@ extern "C" cufsp_status cufsp_likelihood_grad_batched(const cufsp_model_desc *de
     else if (persistent) workers = std::min(workers, 2);
     int dev = 0;
     CUFSP_CUDA_TRY(cudaGetDevice(&dev));
+    // the workers' streams do not wait for the legacy default stream, where the caller's copies of
+    // p0 and the counts were most likely queued
+    CUFSP_CUDA_TRY(upload_fence());
     std::atomic<int> next(0);
     std::vector<cufsp_status> status(workers, CUFSP_SUCCESS);
     std::vector<std::string> msg(workers);

@@ -451,18 +451,18 @@ cufsp_status build_terms(PArnoldi *pa, cufsp_mat *A, const std::vector<double> &
     const int T = (int)shifts.size() + 1;
     if (T > kMaxTerms) return set_error(CUFSP_ERR_UNSUPPORTED, "persistent Arnoldi: more than 63 distinct shifts");
     shifts.push_back(0);
-    // model data on the device (once per generator)
+    // model data on the device (once per generator), in order on st like the build below
     if (!pa->d_nu) {
         CUFSP_CUDA_TRY(cache_alloc((void **)&pa->d_nu, sizeof(int) * (size_t)nr * ns));
-        CUFSP_CUDA_TRY(cudaMemcpy(pa->d_nu, m.nu.data(), sizeof(int) * (size_t)nr * ns, cudaMemcpyHostToDevice));
+        CUFSP_CUDA_TRY(cudaMemcpyAsync(pa->d_nu, m.nu.data(), sizeof(int) * (size_t)nr * ns, cudaMemcpyHostToDevice, st));
         CUFSP_CUDA_TRY(cache_alloc((void **)&pa->d_c, sizeof(double) * nr));
         CUFSP_CUDA_TRY(cache_alloc((void **)&pa->d_rterm, sizeof(int) * nr * 2));
         CUFSP_CUDA_TRY(cache_alloc((void **)&pa->d_d, sizeof(int64_t) * nr));
-        CUFSP_CUDA_TRY(cudaMemcpy(pa->d_d, d.data(), sizeof(int64_t) * nr, cudaMemcpyHostToDevice));
+        CUFSP_CUDA_TRY(cudaMemcpyAsync(pa->d_d, d.data(), sizeof(int64_t) * nr, cudaMemcpyHostToDevice, st));
         if (A->format == CUFSP_FORMAT_KRONECKER) {
             CUFSP_CUDA_TRY(cache_alloc((void **)&pa->d_tables, sizeof(double) * m.tables.size()));
-            CUFSP_CUDA_TRY(cudaMemcpy(pa->d_tables, m.tables.data(), sizeof(double) * m.tables.size(),
-                                      cudaMemcpyHostToDevice));
+            CUFSP_CUDA_TRY(cudaMemcpyAsync(pa->d_tables, m.tables.data(), sizeof(double) * m.tables.size(),
+                                           cudaMemcpyHostToDevice, st));
         }
     }
     TermBuildArgs b;

@@ -5,6 +5,7 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <vector>
 #include <unordered_map>
 
 #include "cufsp_internal.h"
@@ -104,8 +105,9 @@ int stream_grid(int64_t n, int elems_per_thread, int max_ctas) {
 // device.  Work still queued may use a released buffer, so its reuse waits for it: a release that
 // names the stream all uses were ordered on records an event there, and the next owner waits for
 // that event only (other streams keep running); a release without a stream synchronises the
-// buffer's own device.  Idle buffers are kept up to CUFSP_CACHE_MAX_MB (default 1024) per process
-// and returned to the driver by cufsp_cache_trim() or when an allocation of this library fails.
+// buffer's own device.  Idle buffers are kept up to CUFSP_CACHE_MAX_MB (default 1/32 of the device
+// memory, at least 1024) per process and returned to the driver by cufsp_cache_trim() or when an
+// allocation of this library fails.
 namespace {
 struct CachedBlock {
     void *p;
@@ -125,9 +127,19 @@ BufferCache &buffer_cache() {
 }
 size_t cache_cap() {
     static const size_t cap = [] {
-        const char *e = getenv("CUFSP_CACHE_MAX_MB");
-        const long long mb = e ? atoll(e) : 1024;
-        return (size_t)(mb < 0 ? 0 : mb) << 20;
+        if (const char *e = getenv("CUFSP_CACHE_MAX_MB")) {
+            const long long mb = atoll(e);
+            return (size_t)(mb < 0 ? 0 : mb) << 20;
+        }
+        // default: 1/32 of the device memory, at least 1 GB (5.6 GB on a 180 GB part).  Concurrent
+        // gradient workers recycle a few hundred MB each per gradient (checkpoints, bases); a cap
+        // below that sends buffers back through cudaFree, which synchronises the whole device.
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+            cudaGetLastError();
+            total_b = 0;
+        }
+        return std::max<size_t>((size_t)1 << 30, total_b / 32);
     }();
     return cap;
 }
@@ -184,6 +196,43 @@ size_t cache_trim_all() {
     BufferCache &c = buffer_cache();
     std::lock_guard<std::mutex> lk(c.mu);
     return trim_locked(c, -1);
+}
+
+cudaError_t upload_fence() { return cudaStreamSynchronize(cudaStreamLegacy); }
+
+namespace {
+struct PinnedSlots {
+    std::mutex mu;
+    std::vector<double *> free;
+};
+PinnedSlots &pinned_slots() {
+    static PinnedSlots *s = new PinnedSlots();  // never destroyed: no CUDA calls at process exit
+    return *s;
+}
+}  // namespace
+
+double *pinned_slot_get() {
+    PinnedSlots &s = pinned_slots();
+    std::lock_guard<std::mutex> lk(s.mu);
+    if (s.free.empty()) {
+        constexpr int kPage = 512;  // doubles per pinned page (4 KB)
+        double *page = nullptr;
+        if (cudaHostAlloc((void **)&page, sizeof(double) * kPage, cudaHostAllocPortable) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        for (int i = kPage - 1; i >= 0; --i) s.free.push_back(page + i);
+    }
+    double *p = s.free.back();
+    s.free.pop_back();
+    return p;
+}
+
+void pinned_slot_put(double *p) {
+    if (!p) return;
+    PinnedSlots &s = pinned_slots();
+    std::lock_guard<std::mutex> lk(s.mu);
+    s.free.push_back(p);
 }
 
 cudaError_t cache_alloc(void **p, size_t bytes) {
@@ -278,6 +327,17 @@ cufsp_status ReduceScratch::init(int ctas, int k) {
     CUFSP_CUDA_TRY(cache_alloc((void **)&partials, sizeof(double) * (size_t)ctas * k));
     CUFSP_CUDA_TRY(cache_alloc((void **)&counter, sizeof(unsigned int) * 4));
     CUFSP_CUDA_TRY(cudaMemset(counter, 0, sizeof(unsigned int) * 4));
+    CUFSP_CUDA_TRY(upload_fence());
+    return CUFSP_SUCCESS;
+}
+
+cufsp_status ReduceScratch::init(int ctas, int k, cudaStream_t st) {
+    release();
+    max_ctas = ctas;
+    max_k = k;
+    CUFSP_CUDA_TRY(cache_alloc((void **)&partials, sizeof(double) * (size_t)ctas * k));
+    CUFSP_CUDA_TRY(cache_alloc((void **)&counter, sizeof(unsigned int) * 4));
+    CUFSP_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned int) * 4, st));
     return CUFSP_SUCCESS;
 }
 

@@ -65,6 +65,16 @@ void cache_free(void *p);
 void cache_free(void *p, cudaStream_t last_use);
 cudaError_t dev_malloc(void **p, size_t bytes);
 size_t cache_trim_all();
+// cudaMemcpy from pageable memory returns once the data is staged, and cudaMemset once it is
+// queued, both on the legacy default stream, which streams created non-blocking (the batched
+// gradient's workers, the host-buffer action) do not wait for.  Uploads of data that such streams
+// read end with upload_fence(): it returns when the legacy stream's queued work has finished.
+cudaError_t upload_fence();
+// One pinned host double from pages that stay allocated for the process: cudaHostAlloc and
+// cudaFreeHost synchronise the device, which would stall concurrent solves on other streams every
+// time a Krylov driver is created or destroyed.  Null when pinned memory is exhausted.
+double *pinned_slot_get();
+void pinned_slot_put(double *p);
 template <class T>
 cudaError_t dev_malloc(T **p, size_t bytes) {
     return dev_malloc(reinterpret_cast<void **>(p), bytes);
@@ -85,7 +95,8 @@ struct ReduceScratch {
     unsigned int *counter = nullptr;
     int max_ctas = 0;
     int max_k = 0;
-    cufsp_status init(int max_ctas, int max_k);
+    cufsp_status init(int max_ctas, int max_k);                   // counter zeroed before return
+    cufsp_status init(int max_ctas, int max_k, cudaStream_t st);  // counter zeroed in order on st
     void release();
     void release(cudaStream_t last_use);
 };

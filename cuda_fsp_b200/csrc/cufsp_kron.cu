@@ -659,7 +659,8 @@ static void kron_build_rtc(const ModelHost &m, KronData *kd) {
     }
     if (packed.empty()) packed.push_back(0.0);
     if (dev_malloc(&kd->d_rtc_tab, sizeof(double) * packed.size()) != cudaSuccess ||
-        cudaMemcpy(kd->d_rtc_tab, packed.data(), sizeof(double) * packed.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaMemcpy(kd->d_rtc_tab, packed.data(), sizeof(double) * packed.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+        upload_fence() != cudaSuccess) {
         cudaGetLastError();
         kd->rtc_why = "table allocation failed";
         return;
@@ -891,6 +892,11 @@ cufsp_status kron_create(const ModelHost &m, KronData **out) {
         if (e != cudaSuccess) kd->march = false;
     }
     cudaGetLastError();  // a declined fast path leaves no sticky error behind
+    e = upload_fence();
+    if (e != cudaSuccess) {
+        kron_destroy(kd);
+        return cuda_error(e, "kron_create");
+    }
     *out = kd;
     return CUFSP_SUCCESS;
 }

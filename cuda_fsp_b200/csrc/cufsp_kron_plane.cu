@@ -303,6 +303,7 @@ PlaneData *plane_create(const ModelHost &m, const double *d_tables, std::string 
     }
     e = dev_malloc(&pd->d_gtab, sizeof(double2) * g.size());
     if (e == cudaSuccess) e = cudaMemcpy(pd->d_gtab, g.data(), sizeof(double2) * g.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = upload_fence();
     if (e == cudaSuccess && !(pd->h_err = watch_word_alloc(&pd->d_err))) e = cudaErrorMemoryAllocation;
     if (e == cudaSuccess) e = dev_malloc(&pd->d_words, sizeof(double) * (size_t)Q * pd->wa.nwp);
     if (e != cudaSuccess) {

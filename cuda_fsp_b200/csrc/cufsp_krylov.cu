@@ -719,6 +719,7 @@ extern "C" cufsp_status cufsp_expv_create(int64_t n, int m, double tol, int iop,
     cudaError_t e = cache_alloc((void **)&E->W, sizeof(double) * (size_t)n * (size_t)(m + 1));
     if (e == cudaSuccess) e = cache_alloc((void **)&E->d_state, E->state_bytes);
     if (e == cudaSuccess) e = cudaMemset(E->d_state, 0, E->state_bytes);
+    if (e == cudaSuccess) e = upload_fence();
     if (e != cudaSuccess) {
         cufsp_expv_destroy(E);
         return cuda_error(e, "cufsp_expv_create");
@@ -731,8 +732,7 @@ extern "C" cufsp_status cufsp_expv_create(int64_t n, int m, double tol, int iop,
     E->ks.avnorm = E->ks.beta + 1;
     E->ks.btol = E->ks.beta + 2;
     E->ks.flag = reinterpret_cast<int *>(E->ks.beta + 4);
-    if (cudaHostAlloc((void **)&E->h_btol, sizeof(double), cudaHostAllocDefault) != cudaSuccess) {
-        cudaGetLastError();
+    if (!(E->h_btol = pinned_slot_get())) {
         cufsp_expv_destroy(E);
         return set_error(CUFSP_ERR_ALLOC, "cufsp_expv_create: pinned allocation failed");
     }
@@ -762,7 +762,9 @@ extern "C" cufsp_status cufsp_expv_destroy(cufsp_expv *E) {
         E->rs.release();
     }
     if (E->cap_stream) cudaStreamDestroy(E->cap_stream);
-    if (E->h_btol) cudaFreeHost(E->h_btol);
+    // every copy from h_btol completed inside the call that issued it (each pass ends with a blocking
+    // read of its state block), so the slot is free for the next driver
+    pinned_slot_put(E->h_btol);
     delete E;
     return CUFSP_SUCCESS;
 }

@@ -284,6 +284,11 @@ cufsp_status sparse_create(const ModelHost &m, SparseData **out) {
     // P must be finite for the action to be well defined.
     std::string why;
     sparse_build_rtc(m, sd, why);
+    if (upload_fence() != cudaSuccess) {
+        cudaGetLastError();
+        sparse_destroy(sd);
+        return set_error(CUFSP_ERR_CUDA, "sparse_create: upload failed");
+    }
     sd->describe = sd->rtc ? "sparse: propensity table, kernel specialised for the network and box (NVRTC, sm_100a), " +
                                  std::to_string(sd->rtc_grid) + " CTAs x 256 threads"
                            : "sparse: propensity table, k_sparse_mv (" + why + ")";

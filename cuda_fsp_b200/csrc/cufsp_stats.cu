@@ -107,12 +107,15 @@ extern "C" cufsp_status cufsp_loglik(int64_t n, const double *d_p, int64_t block
                                      double *out, cufsp_stream_t stream) {
     if (!d_p || !d_counts || !out || n < 1 || block < 1 || n % block != 0 || block > 2147483647LL)
         return set_error(CUFSP_ERR_INVALID_ARG, "cufsp_loglik: bad argument");
+    // scratch in order on the caller's stream: no device-wide synchronisation, so concurrent callers
+    // on other streams (the batched gradient's workers) keep running
+    cudaStream_t st = (cudaStream_t)stream;
     ReduceScratch rs;
     const int ctas = device_info().sm_count * 4;
-    cufsp_status s = rs.init(ctas, 1);
+    cufsp_status s = rs.init(ctas, 1, st);
     double *d_out = nullptr;
-    if (s == CUFSP_SUCCESS && dev_malloc(&d_out, sizeof(double)) != cudaSuccess)
-        s = set_error(CUFSP_ERR_ALLOC, "cufsp_loglik: cudaMalloc");
+    if (s == CUFSP_SUCCESS && cache_alloc((void **)&d_out, sizeof(double)) != cudaSuccess)
+        s = set_error(CUFSP_ERR_ALLOC, "cufsp_loglik: device allocation failed");
     if (s == CUFSP_SUCCESS) {
         const int64_t nk = n / block;
         const int g = stream_grid(nk, 1, ctas);
@@ -123,8 +126,8 @@ extern "C" cufsp_status cufsp_loglik(int64_t n, const double *d_p, int64_t block
         if (e == cudaSuccess) e = cudaStreamSynchronize((cudaStream_t)stream);
         if (e != cudaSuccess) s = cuda_error(e, "cufsp_loglik");
     }
-    if (d_out) cudaFree(d_out);
-    rs.release();
+    if (d_out) cache_free(d_out, st);
+    rs.release(st);
     return s;
 }
 
@@ -238,6 +241,7 @@ extern "C" cufsp_status cufsp_ssa(const cufsp_model_desc *desc, const double *co
     if (e == cudaSuccess) e = cudaMemcpy(d_x0, x0, sizeof(int) * m.ns, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(d_times, times, sizeof(double) * n_times, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(d_err, 0, sizeof(int));
+    if (e == cudaSuccess) e = upload_fence();
     int herr = 0;
     if (e == cudaSuccess) {
         a.tables = d_tab;

@@ -317,7 +317,9 @@ cufsp_status cufsp_likelihood_grad(cufsp_mat *A, const double *coefs, int n_time
 /* The same gradient for n_sets parameter sets (coefs: host [n_sets][n_reactions]; logL: host [n_sets];
  * grad: host [n_sets][n_reactions]) sharing times, p0 and counts.  `workers` host threads, each with
  * its own KRONECKER generator built from desc, stream and workspaces, overlap their solves on the
- * GPU.  No counterpart in the reference.  Synchronous. */
+ * GPU.  The workers' streams are non-blocking: the call first waits for the work queued on the
+ * legacy default stream (the usual producer of d_p0 and d_counts); inputs written on other streams
+ * must be complete before the call.  No counterpart in the reference.  Synchronous. */
 cufsp_status cufsp_likelihood_grad_batched(const cufsp_model_desc *desc, int n_sets, const double *coefs,
                                            int n_times, const double *times, const double *d_p0, int64_t block,
                                            const double *d_counts, int m, double tol, int workers, double *logL,

@@ -5,7 +5,7 @@ benchmark legs run, where step counts, grids, launch shapes and rounding differ:
   * batched Krylov over gene_batch(256) instances whose mRNA bounds span 63..255 (t = 30), and the
     single-instance path on the same instances, each against a tol = 1e-13 oracle solution;
   * the adjoint gradient on the 131,072-state gene box against forward sensitivities integrated by
-    the oracle's Krylov expv;
+    the oracle's Krylov expv, and the batched gradient (concurrent workers) against single calls;
   * the BDF path on the 131,072-state time-varying gene model against the oracle's BDF;
   * Krylov steps through the overwrite-form plane kernel on a 128^3 box of the 255^3 workload's
     network (above the persistent pass's 2^20 states) against the oracle.
@@ -89,6 +89,32 @@ def test_c5_gradient_on_full_gene_box(cuda):
     assert abs(ll - ll_ref) <= 1e-8 * abs(ll_ref)
     for r in rates:
         assert abs(g[r] - g_ref[r]) <= GRAD_RTOL * abs(g_ref[r]), (r, g[r], g_ref[r])
+
+
+def test_c5_batched_gradients_equal_single_on_full_gene_box(cuda, monkeypatch):
+    """cufsp_likelihood_grad_batched at the gradient leg's size (131,072 states, 8 times in [1, 60],
+    rates within half a decade of nominal): concurrent workers on non-blocking streams, several sets
+    per worker on the worker's reused generator and recycled buffers, give each set's single-call
+    result.  With CUFSP_GRAD_SM_SHARE=0 every worker's persistent pass takes the whole GPU, as a single
+    call does, so both paths do the same arithmetic in the same order (all reductions are fixed-order)
+    and must agree to the last bits: a reduction that read another worker's scratch, or a counter
+    zeroed out of order with the worker's stream, shows up as a difference.  (With the default SM
+    shares the passes run on fewer CTAs and round differently; the Krylov step control can then take
+    another accept/reject decision, and cells whose probability is below the absolute tolerance move
+    log max(1e-44, p) by up to ~70 each: a tolerance effect, not a parity one.)"""
+    monkeypatch.setenv("CUFSP_GRAD_SM_SHARE", "0")
+    m = models.gene_expression((1, 1, 1, 127, 127), time_varying=False)
+    times = np.geomspace(1.0, 60.0, 8)
+    snaps = generate_data(m, times, [0, 0, 0, 0, 0], 1000, seed=20261205)
+    counts, outside = histograms(snaps, m.bounds, n_marginal=3)
+    L = Likelihood(m, times, counts, outside=outside, n_marginal=3, kry_tol=1e-8)
+    rng = np.random.default_rng(7)
+    sets = np.stack([m.coefs(0) * 10.0 ** rng.uniform(-0.5, 0.5, m.nr) for _ in range(6)])
+    ll_b, g_b = L.gradient_batched(sets, workers=2)
+    for i in range(len(sets)):
+        ll, g = L.gradient(sets[i])
+        assert abs(ll_b[i] - ll) <= 1e-13 * abs(ll), (i, ll_b[i], ll)
+        assert np.abs(g_b[i] - g).max() <= 1e-12 * np.abs(g).max(), (i, np.abs(g_b[i] - g).max())
 
 
 def test_c2_bdf_on_full_gene_box(cuda):
