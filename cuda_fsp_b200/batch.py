@@ -249,7 +249,7 @@ def solve_sharded(models_, t_final: float, rank: int, world: int, m: int = 30, t
     return out
 
 
-def gradient_sharded(likelihood, coef_sets, rank: int, world: int, workers: int = 2, group=None, grad_fn=None):
+def gradient_sharded(likelihood, coef_sets, rank: int, world: int, workers: int = 4, group=None, grad_fn=None):
     """d log L / d log c for many parameter sets over several GPUs: the sets are split into `world`
     contiguous blocks, each rank computes its block (Likelihood.gradient_batched, or grad_fn(sets) ->
     (logL [k], grad [k, nr]) in host tests), and one all_gather of the packed (log L, gradient) rows
