@@ -107,6 +107,21 @@ def test_oracle_expv_matches_scipy_expm_multiply():
     assert np.abs(w - ws).sum() <= 1e-8
 
 
+@pytest.mark.parametrize("m_dim,q", [(30, 2), (60, 3), (60, 4)])
+def test_oracle_iop_expv_matches_scipy_on_stiff_network(m_dim, q):
+    """Incomplete orthogonalisation (src/KryExpvFSP.cu:74, q vectors) as the 255^3 expmv leg runs it
+    (m = 60, q = 3) and as the reference's own test does (m = 30, q = 2), on a 21^3 box of the same
+    stiff 3-species network to t = 0.2: within the Krylov tolerance of SciPy's expm_multiply."""
+    import scipy.sparse.linalg as spla
+    m = models.mass_action_3(bounds=(20, 20, 20))
+    A = oracle.assemble_model(m)
+    c = m.coefs(0)
+    w, st, rc = oracle.expv(A, c, 0.2, m.p0(), m=m_dim, tol=1e-8, iop=True, q_iop=q)
+    assert rc == 0 and st["t_now"] == 0.2
+    ws = spla.expm_multiply(A.to_scipy(c) * 0.2, m.p0())
+    assert np.abs(w - ws).sum() <= 1e-8
+
+
 def test_oracle_mass_conservation_reference_case():
     """tests/test_kry_expv.cu:80-110: toggle on 257^2 states, t = 8 h, m = 30, tol 1e-8, IOP q = 2;
     |1 - sum v| <= 1e-10."""
