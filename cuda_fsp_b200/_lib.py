@@ -141,6 +141,7 @@ SIGNATURES = {
     "cufsp_expv_final_time_reached": [_P, _IP],
     "cufsp_expv_get_stats": [_P, C.POINTER(ExpvStats)],
     "cufsp_expm_host": [C.c_int, _DP, _DP],
+    "cufsp_expm_blocktri_host": [C.c_int, C.c_int, _DP, _DP],
     "cufsp_bdf_create": [_P, _DP, C.c_double, C.c_double, C.c_int, C.POINTER(_P)],
     "cufsp_bdf_destroy": [_P],
     "cufsp_bdf_set_options": [_P, C.c_double, C.c_double, C.c_double, C.c_int64],

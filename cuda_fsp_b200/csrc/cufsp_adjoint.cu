@@ -437,7 +437,7 @@ extern "C" cufsp_status cufsp_likelihood_grad(cufsp_mat *A, const double *coefs,
                     for (int jj = 0; jj < mbf; ++jj)
                         for (int ii = 0; ii < mbf; ++ii)
                             Xb[(mbb + ii) + (size_t)(mbb + jj) * K] = tau * F.H[jj + (size_t)ii * mbf];  // H^T
-                    s = expm_pade13(K, Xb.data(), Fb.data());
+                    s = expm_pade13_blocktri(mbb, mbf, Xb.data(), Fb.data());
                     if (s != CUFSP_SUCCESS) return s;
                     // uhat_b = sum_a W[a][b] rho_b[a] Ub_a
                     coefm.assign((size_t)mbb * mbf, 0.0);

@@ -202,6 +202,8 @@ struct KrylovStep {
 
 // Host-side dense exponential (cufsp_expm.cpp).
 cufsp_status expm_pade13(int k, const double *A, double *F);
+// exp of [[A11, A12], [0, A22]] (k1 + k2 square, column-major; the lower-left block is not read)
+cufsp_status expm_pade13_blocktri(int k1, int k2, const double *A, double *F);
 
 }  // namespace cufsp
 

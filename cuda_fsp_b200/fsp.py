@@ -339,4 +339,18 @@ def expm(a: np.ndarray) -> np.ndarray:
     return F
 
 
-__all__ = ["MatrixFormat", "FSPMat", "KryExpvFSP", "CufspError", "num_states", "get_states", "expm"]
+def expm_blocktri(a: np.ndarray, k1: int) -> np.ndarray:
+    """exp of a block upper-triangular matrix [[A11, A12], [0, A22]] with A11 of size k1 (host; the
+    lower-left block of `a` is not read): the same Pade(13,13) method with three block products per
+    matrix product."""
+    lib = _lib.load()
+    A = np.asfortranarray(np.asarray(a, np.float64))
+    k = A.shape[0]
+    F = np.empty_like(A, order="F")
+    _lib.check(lib, lib.cufsp_expm_blocktri_host(int(k1), k - int(k1), A.ctypes.data_as(C.POINTER(C.c_double)),
+                                                 F.ctypes.data_as(C.POINTER(C.c_double))), "cufsp_expm_blocktri_host")
+    return F
+
+
+__all__ = ["MatrixFormat", "FSPMat", "KryExpvFSP", "CufspError", "num_states", "get_states", "expm",
+           "expm_blocktri"]

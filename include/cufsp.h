@@ -384,6 +384,11 @@ cufsp_status cufsp_batch_describe(const cufsp_batch *B, char *buf, size_t len);
 /* Dense exponential of a k x k column-major host matrix by scaling-and-squaring Pade(13,13)
  * (replaces arma::expmat at src/KryExpvFSP.cu:125). */
 cufsp_status cufsp_expm_host(int k, const double *A, double *F);
+/* The same for a block upper-triangular (k1 + k2) x (k1 + k2) matrix [[A11, A12], [0, A22]] (the
+ * lower-left block of A is not read; F's is zero), three block products per matrix product instead
+ * of eight.  The adjoint gradient's Van Loan exponentials have this form.  No counterpart in the
+ * reference. */
+cufsp_status cufsp_expm_blocktri_host(int k1, int k2, const double *A, double *F);
 
 /* ---- vector helpers (device) ------------------------------------------------------------- */
 /* sum of x (deterministic order); result written to host *out; synchronises `stream`. */

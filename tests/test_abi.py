@@ -66,6 +66,25 @@ def test_host_expm_matches_oracle(built):
         assert np.abs(expm(A) - E).max() <= 1e-12 * np.abs(E).max()
 
 
+def test_host_blocktri_expm_matches_full(built):
+    """The block upper-triangular exponential (the adjoint's Van Loan matrices [[tau G, tau z y^T],
+    [0, tau H^T]]) equals the full one and SciPy's, for blocks that are and are not multiples of the
+    8-wide padding, small and large norms; the lower-left block is never read."""
+    import scipy.linalg as sla
+    from cuda_fsp_b200.fsp import expm, expm_blocktri
+    rng = np.random.default_rng(4)
+    for k1, k2, s in [(30, 30, 0.5), (29, 31, 3.0), (1, 1, 1.0), (5, 40, 0.2), (40, 3, 20.0), (8, 8, 0.0)]:
+        A = rng.standard_normal((k1 + k2, k1 + k2)) * s
+        A[k1:, :k1] = 0.0
+        E = sla.expm(A)
+        Ab = A.copy()
+        Ab[k1:, :k1] = np.nan
+        F = expm_blocktri(Ab, k1)
+        assert np.all(F[k1:, :k1] == 0.0)
+        assert np.abs(F - E).max() <= 1e-12 * np.abs(E).max()
+        assert np.abs(F - expm(A)).max() <= 1e-13 * np.abs(E).max()
+
+
 def test_invalid_models_rejected_before_any_device_work(built):
     m = models.toggle((31, 31))
     with pytest.raises(_lib.CufspError) as e:
