@@ -71,6 +71,7 @@ def test_host_blocktri_expm_matches_full(built):
     [0, tau H^T]]) equals the full one and SciPy's, for blocks that are and are not multiples of the
     8-wide padding, small and large norms; the lower-left block is never read."""
     import scipy.linalg as sla
+    from cuda_fsp_b200 import CufspError
     from cuda_fsp_b200.fsp import expm, expm_blocktri
     rng = np.random.default_rng(4)
     for k1, k2, s in [(30, 30, 0.5), (29, 31, 3.0), (1, 1, 1.0), (5, 40, 0.2), (40, 3, 20.0), (8, 8, 0.0)]:
@@ -83,6 +84,14 @@ def test_host_blocktri_expm_matches_full(built):
         assert np.all(F[k1:, :k1] == 0.0)
         assert np.abs(F - E).max() <= 1e-12 * np.abs(E).max()
         assert np.abs(F - expm(A)).max() <= 1e-13 * np.abs(E).max()
+    with pytest.raises(CufspError) as ei:  # an empty diagonal block is an argument error
+        expm_blocktri(np.eye(4), 0)
+    assert ei.value.name == "CUFSP_ERR_INVALID_ARG"
+    with pytest.raises(CufspError) as ei:  # NaN/Inf in the blocks that are read
+        A = np.eye(6)
+        A[0, 5] = np.inf
+        expm_blocktri(A, 3)
+    assert ei.value.name == "CUFSP_ERR_NONFINITE"
 
 
 def test_invalid_models_rejected_before_any_device_work(built):
