@@ -36,6 +36,29 @@ def test_indexing_matches_reference_host_code(bounds):
         assert oracle.state2indx(s, b) == i
 
 
+def test_oracle_matches_committed_reference_vectors():
+    """The same pins as the two tests around this one, against vectors the reference's own host code
+    produced (tests/golden/reference_host.npz, written by tests/golden/make_reference_vectors.py
+    through the compiled shim), so that they hold where the shim cannot be built."""
+    from pathlib import Path
+    import sys
+    sys.path.insert(0, str(Path(__file__).parent / "golden"))
+    from make_reference_vectors import BOUNDS, golden_models
+    g = np.load(Path(__file__).parent / "golden" / "reference_host.npz")
+    for k, bounds in enumerate(BOUNDS):
+        b = np.asarray(bounds, np.int32)
+        assert np.array_equal(g[f"box{k}_bounds"], b)
+        assert oracle.num_states(b) == int(g[f"box{k}_n"])
+        idx = g[f"box{k}_idx"]
+        st = oracle.get_states(b)
+        assert np.array_equal(st[idx], g[f"box{k}_states"])
+        assert np.array_equal(g[f"box{k}_state2indx"], idx)
+        assert all(oracle.state2indx(s, b) == i for s, i in zip(g[f"box{k}_states"], idx))
+    for name, m in golden_models().items():
+        assert np.array_equal(g[f"{name}_vals"], m.tables), name
+        assert np.array_equal(g[f"{name}_offsets"], -m.nu), name
+
+
 def test_factor_table_layout_matches_reference():
     """fspmat_sdkron_fill_host_data (src/fspmat_kron_kernels.cu:170-190) fills the same table
     layout the product consumes, and its offsets are -nu."""
