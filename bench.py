@@ -897,7 +897,7 @@ def main():
                     default=None,
                     help="run one leg alone (profiling runs; see run_leg)")
     ap.add_argument("--box", default=None, help="box bounds of the leg, comma separated")
-    ap.add_argument("--workers", type=int, default=2, help="host workers of the gradbatch leg")
+    ap.add_argument("--workers", type=int, default=4, help="host workers of the gradbatch leg")
     ap.add_argument("--krylov-m", type=int, default=30, help="Krylov dimension of the krylov leg")
     ap.add_argument("--iop", type=int, default=0, help="incomplete orthogonalisation depth q of the krylov leg (0: full)")
     args = ap.parse_args()
